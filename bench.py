@@ -1,0 +1,410 @@
+"""Benchmark of the sm_100a equi-hash-join on the large 1:1 foreign-key workload.
+
+Workload (one "step" = one pass of the hot path over one probe batch):
+  build 16M rows: unique int64 keys (seeded 40-bit Feistel permutation of 0..2^40) + two int64
+  payloads; probe 64M rows: int64 keys drawn uniformly from the build keys (every probe matches
+  once) + one int64 payload; output per match: probe rid, build rid (int32), probe payload and
+  both build payloads (32 bytes).
+
+Reported (one JSON line on rank 0):
+  value     probe Mtuples/s of the probe phase (probe + payload gather + output write) against a
+            device-resident table (the BUILD_PROBE pattern: build once, probe many), inputs
+            resident in HBM; all ranks' probe rows / max-over-ranks time;
+  e2e       the same metric for the one-shot join through the C ABI from pinned host buffers:
+            H2D of all inputs + build + probe/gather + D2H of the whole output, per step;
+  roofline  algorithmic bytes of the probe phase per launch / the probe kernel's average
+            CUDA-event duration, against the measured HBM copy bandwidth;
+  cpu_baseline  the CPU oracle join (all host threads) on the same workload.
+Multi-GPU (torchrun): every rank builds the same table (a replicated build, the reference's
+broadcast-join shape) and probes its own 64M-row shard: weak scaling, no data-path collective.
+
+--impl reference: the CPU join (the oracle restatement of the reference's algorithm; the
+reference itself cannot be built here) timed on the host cores on the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+NOMINAL_HBM_GBS = 8000.0
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="sj", choices=["sj", "reference"])
+    ap.add_argument("--n-build", type=int, default=16 << 20)
+    ap.add_argument("--n-probe", type=int, default=64 << 20)
+    ap.add_argument("--seed", type=int, default=1)
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--cpu-steps", type=int, default=2)
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--partition-bits", type=int, default=0)
+    return ap.parse_args()
+
+
+def measured_peak():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            d = json.loads(p.read_text())
+            return float(d["hbm_gbs"]), "measured (MEASURED_PEAKS.json hbm_gbs)"
+        except Exception:
+            pass
+    return FALLBACK_HBM_GBS, "fallback 6.65 TB/s"
+
+
+def profile_traffic(kernel: str):
+    """DRAM bytes per launch of `kernel` from the committed ncu summary, if any."""
+    p = ROOT / "profiles" / "traffic.json"
+    if not p.exists():
+        return None, None
+    try:
+        d = json.loads(p.read_text())
+        e = d.get(kernel)
+        return (float(e["bytes_per_launch"]), e.get("source")) if e else (None, None)
+    except Exception:
+        return None, None
+
+
+class ClockSampler:
+    """nvidia-smi samples during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+        self.t = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            if self.t:
+                self.t.join(timeout=2)
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in self.lines:
+            f = [x.strip() for x in l.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def workload_desc(nb, np_):
+    return (f"large 1:1 FK equi-join: build {nb} rows unique int64 keys (seeded Feistel over 0..2^40) "
+            f"+ 2 int64 payloads; probe {np_} rows int64 keys drawn from the build keys (all match) "
+            f"+ 1 int64 payload; output probe rid, build rid, 3 payloads (32 B/row)")
+
+
+def alg_bytes_probe_phase(inp) -> int:
+    """Compulsory bytes of the probe phase: probe keys + probe payloads read once, build payloads
+    read once, every output byte written once (table traffic is not counted)."""
+    probe_in = inp.probe_keys.nbytes + sum(c.nbytes for c in inp.probe_payload)
+    build_pay = sum(c.nbytes for c in inp.build_payload)
+    out = inp.n_probe * inp.output_row_bytes()  # every probe row matches once
+    return probe_in + build_pay + out
+
+
+# --------------------------------------------------------------------------------------------
+# CPU join (oracle) timing
+# --------------------------------------------------------------------------------------------
+def cpu_join_seconds(inp, threads):
+    from oracle import oracle as O
+    t0 = time.perf_counter()
+    r = O.hash_join(inp.build_keys, inp.probe_keys, probe_payload=inp.probe_payload,
+                    build_payload=inp.build_payload, threads=threads, capacity=inp.n_probe)
+    dt = time.perf_counter() - t0
+    assert r.rows == inp.n_probe
+    return dt
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    from oracle import oracle as O
+    from sirius_b200 import datagen as D
+    O.build()
+    inp = D.large(args.seed, args.n_build, args.n_probe)
+    threads = O.default_threads()
+    for _ in range(max(0, args.warmup)):
+        cpu_join_seconds(inp, threads)
+    times = [cpu_join_seconds(inp, threads) for _ in range(max(1, args.steps))]
+    total = sum(times)
+    value = args.n_probe * len(times) / total / 1e6
+    line = {
+        "impl": "reference", "metric": "join probe Mtuples/s", "value": round(value, 3), "unit": "Mtuples/s",
+        "n_gpus": args.gpus, "steps": len(times), "warmup": args.warmup,
+        "ms_per_step": round(1e3 * total / len(times), 3), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "int64", "data": "synthetic (seeded)",
+        "config": {"workload": workload_desc(args.n_build, args.n_probe), "build_rows": args.n_build,
+                   "probe_rows": args.n_probe},
+        "cpu_baseline": {"value": round(value, 3), "unit": "Mtuples/s", "cores": threads, "kind": "port",
+                         "sample": "full workload per step: one-shot CPU hash join (build + probe + payload "
+                                   "gather into host arrays) by the oracle's multithreaded C join; the "
+                                   "reference (libcudf) cannot be built or run here"},
+        "e2e": {"value": round(value, 3), "unit": "Mtuples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# --------------------------------------------------------------------------------------------
+# GPU
+# --------------------------------------------------------------------------------------------
+def run_sj(args):
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    else:
+        torch.cuda.set_device(0)
+    dev = torch.device("cuda", torch.cuda.current_device())
+
+    from sirius_b200 import datagen as D
+    from sirius_b200 import join as J
+    from sirius_b200 import _lib
+
+    _lib.load()
+    # every rank: the same build side; its own probe shard (seed stream offset by rank)
+    inp = D.large(args.seed, args.n_build, args.n_probe)
+    if rank > 0:
+        # same build side; this rank's probe shard drawn from it with the rank's own stream
+        rng = np.random.default_rng([args.seed, rank])
+        inp.probe_keys = inp.build_keys[rng.integers(0, args.n_build, args.n_probe)]
+        inp.probe_payload = [rng.integers(-2**63, 2**63 - 1, args.n_probe, dtype=np.int64, endpoint=True)]
+    bk = torch.from_numpy(inp.build_keys).to(dev)
+    pk = torch.from_numpy(inp.probe_keys).to(dev)
+    bp = [torch.from_numpy(c).to(dev) for c in inp.build_payload]
+    pp = [torch.from_numpy(c).to(dev) for c in inp.probe_payload]
+    stream = torch.cuda.current_stream()
+
+    # ---- build (timed separately) ----
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t_build = []
+    for i in range(3):
+        torch.cuda.synchronize()
+        ev0.record()
+        tb = J.HashTable(bk, partition_bits=args.partition_bits)
+        ev1.record()
+        torch.cuda.synchronize()
+        t_build.append(ev0.elapsed_time(ev1))
+        if i < 2:
+            tb.close()
+    table = tb
+    info = table.info()
+
+    out = J.allocate_output(args.n_probe, pp, bp, dev)
+    d_count = torch.zeros(1, dtype=torch.int64, device=dev)
+
+    def step():
+        table.probe_gather(pk, None, pp, bp, capacity=args.n_probe, out=out, d_count=d_count, sync=False)
+
+    for _ in range(max(3, args.warmup)):
+        step()
+    torch.cuda.synchronize()
+    got = int(d_count.item())
+    assert got == args.n_probe, f"probe produced {got} rows, expected {args.n_probe}"
+    # correctness spot check of the timed configuration (full size, size-independent properties)
+    sample = torch.randint(0, args.n_probe, (1 << 16,), device=dev)
+    prid = out.probe_rid[sample].long()
+    brid = out.build_rid[sample].long()
+    assert torch.equal(pk[prid], bk[brid]), "joined keys differ"
+    assert torch.equal(out.build_payload[0][sample], bp[0][brid])
+    assert torch.equal(out.probe_payload[0][sample], pp[0][prid])
+
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    with ClockSampler(dev.index) as clk:
+        t_all0 = torch.cuda.Event(enable_timing=True)
+        t_all1 = torch.cuda.Event(enable_timing=True)
+        t_all0.record()
+        for i in range(args.steps):
+            starts[i].record()
+            step()
+            ends[i].record()
+        t_all1.record()
+        torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    total_ms = t_all0.elapsed_time(t_all1)
+    per_launch = [s.elapsed_time(e) for s, e in zip(starts, ends)]
+    t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    max_ms = float(t.item())
+    rows_all = args.n_probe * args.steps * world
+    value = rows_all / (max_ms / 1e3) / 1e6
+    clocks = clk.summary()
+
+    # ---- e2e: one-shot join through the C ABI from pinned host buffers ----
+    e2e = None
+    if args.e2e_steps > 0:
+        pin = lambda a: torch.from_numpy(a).pin_memory()  # noqa: E731
+        h_bk, h_pk = pin(inp.build_keys), pin(inp.probe_keys)
+        h_bp = [pin(c) for c in inp.build_payload]
+        h_pp = [pin(c) for c in inp.probe_payload]
+        d_bk, d_pk = torch.empty_like(bk), torch.empty_like(pk)
+        d_bp = [torch.empty_like(c) for c in bp]
+        d_pp = [torch.empty_like(c) for c in pp]
+        h_out = [torch.empty(args.n_probe, dtype=torch.int32).pin_memory() for _ in range(2)]
+        h_out += [torch.empty(args.n_probe, dtype=c.dtype).pin_memory() for c in pp + bp]
+        h2d = sum(x.numel() * x.element_size() for x in [h_bk, h_pk] + h_bp + h_pp)
+        d2h = sum(x.numel() * x.element_size() for x in h_out)
+
+        def e2e_step():
+            d_bk.copy_(h_bk, non_blocking=True)
+            d_pk.copy_(h_pk, non_blocking=True)
+            for d, h in zip(d_bp + d_pp, h_bp + h_pp):
+                d.copy_(h, non_blocking=True)
+            with J.HashTable(d_bk) as tt:
+                tt.probe_gather(d_pk, None, d_pp, d_bp, capacity=args.n_probe, out=out, d_count=d_count,
+                                sync=False)
+                srcs = [out.probe_rid, out.build_rid] + out.probe_payload + out.build_payload
+                for h, s in zip(h_out, srcs):
+                    h.copy_(s, non_blocking=True)
+                torch.cuda.synchronize()
+
+        e2e_step()
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        w0 = time.perf_counter()
+        e0.record()
+        for _ in range(args.e2e_steps):
+            e2e_step()
+        e1.record()
+        torch.cuda.synchronize()
+        e_ms = e0.elapsed_time(e1)
+        wall_ms = (time.perf_counter() - w0) * 1e3
+        te = torch.tensor([max(e_ms, wall_ms)], dtype=torch.float64, device=dev)
+        if world > 1:
+            dist.all_reduce(te, op=dist.ReduceOp.MAX)
+        e_max = float(te.item())
+        assert int(d_count.item()) == args.n_probe
+        e2e = {"value": round(args.n_probe * args.e2e_steps * world / (e_max / 1e3) / 1e6, 3),
+               "unit": "Mtuples/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+               "ms_per_step": round(e_max / args.e2e_steps, 3),
+               "what": "one-shot join from pinned host buffers: H2D of all inputs, sj_build, "
+                       "sj_probe_gather, D2H of the whole output"}
+
+    # ---- roofline of the probe kernel ----
+    alg = alg_bytes_probe_phase(inp)
+    launch_ms = statistics.mean(per_launch)
+    peak, peak_src = measured_peak()
+    achieved = alg / (launch_ms / 1e3) / 1e9
+    traffic, traffic_src = profile_traffic("probe_distinct_kernel")
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu and args.cpu_steps > 0:
+        from oracle import oracle as O
+        O.build()
+        threads = O.default_threads()
+        ts = [cpu_join_seconds(inp, threads) for _ in range(args.cpu_steps)]
+        cpu = {"value": round(args.n_probe / statistics.median(ts) / 1e6, 3), "unit": "Mtuples/s",
+               "cores": threads, "kind": "port",
+               "sample": f"full workload, {len(ts)} one-shot CPU joins (build + probe + gather into host "
+                         f"arrays), median {statistics.median(ts):.3f} s; oracle multithreaded C join"}
+
+    if rank == 0:
+        line = {
+            "metric": "join probe Mtuples/s", "value": round(value, 3), "unit": "Mtuples/s", "n_gpus": world,
+            "steps": args.steps, "warmup": max(3, args.warmup), "ms_per_step": round(max_ms / args.steps, 4),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64",
+            "data": "synthetic (seeded numpy PCG64 / Feistel keys)",
+            "config": {"workload": workload_desc(args.n_build, args.n_probe), "build_rows": args.n_build,
+                       "probe_rows": args.n_probe, "parallelism": f"replicated build, probe sharded x{world}",
+                       "l2": "no flush: every step streams 1 GiB of probe input and writes 2 GiB of output, "
+                             "both larger than the 126 MB L2",
+                       "table": {"layout": "DISTINCT" if info.layout == 1 else "GROUPED",
+                                 "slot": "PACKED64" if info.slot_kind == 0 else "WIDE128",
+                                 "slots": int(info.num_slots), "rid_bits": int(info.rid_bits),
+                                 "bytes": int(info.device_bytes), "partition_bits": int(info.partition_bits)},
+                       "t_build_ms": round(min(t_build), 3)},
+            "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                         "frac": round(achieved / peak, 4), "traffic": traffic,
+                         "kernel": "probe_distinct_kernel", "alg_bytes_per_launch": int(alg),
+                         "launch_ms": round(launch_ms, 4), "peak_source": peak_src,
+                         "frac_of_nominal_8TBs": round(achieved / NOMINAL_HBM_GBS, 4),
+                         "traffic_source": traffic_src},
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "gpu_launches": args.steps,
+            "clocks": clocks,
+        }
+        print(json.dumps(line), flush=True)
+    table.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_sj(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,237 @@
+/*
+ * sj_join.h — C ABI of the B200 (sm_100a) equi-hash-join.
+ *
+ * This is the drop-in boundary that replaces the three cuDF calls inside Sirius's
+ * physical hash-join operator, `sirius_physical_hash_join::execute`
+ * (src/op/sirius_physical_hash_join.cpp:1527-1955):
+ *
+ *   build   cudf::hash_join(keys, compare_nulls(), stream)           (:1620)
+ *           cudf::distinct_hash_join(keys, UNEQUAL, 0.5, stream)      (:1614-1615, :1852)
+ *   probe   hash_join::inner_join(probe_keys, {}, stream)             (:1688)
+ *           distinct_hash_join::inner_join(probe_keys, stream)        (:1671)
+ *           cudf::inner_join(left_keys, right_keys, nulls, stream)    (:1872)
+ *   gather  gather_join_output -> cudf::gather(...) x2                (:1299-1359, :1336, :1348)
+ *
+ * Conventions (the cuDF ones the operator already uses):
+ *   - a column is a contiguous array of fixed-width values plus an optional validity bitmask of
+ *     32-bit words; bit (validity_offset + i) % 32 of word (validity_offset + i) / 32 set means
+ *     row i is valid (not NULL);
+ *   - row ids are int32 (cudf::size_type, src/op/sirius_physical_hash_join.cpp:1305-1306);
+ *   - "probe" = left = input_batches[0], "build" = right = input_batches[1]
+ *     (src/op/sirius_physical_hash_join.cpp:1157-1158);
+ *   - output columns are [probe payload columns..., build payload columns...], the order
+ *     gather_join_output assembles (src/op/sirius_physical_hash_join.cpp:1350-1355).
+ *
+ * Every pointer argument named d_* or carrying column data is device memory on the current
+ * device. Every call is stream-ordered on the given stream unless its comment says it
+ * synchronizes. Calls on distinct tables are thread-safe; probes of one built table may run
+ * concurrently from many threads and streams (the BUILD_PROBE pattern, one writer then many
+ * readers, src/op/sirius_physical_hash_join.cpp:1585-1588, :1624).
+ *
+ * Errors are returned as sj_status; a human-readable message for the last failing call on the
+ * calling thread is available from sj_last_error(). No call throws across the ABI.
+ */
+#ifndef SJ_JOIN_H
+#define SJ_JOIN_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Same export style as Sirius's FFI layer (SIRIUS_FFI_EXPORT, src/include/sirius_ffi.hpp:37). */
+#ifndef SJ_EXPORT
+#define SJ_EXPORT __attribute__((visibility("default")))
+#endif
+
+/* Binary-compatible with cudaStream_t; 0 is the legacy default stream. */
+typedef struct CUstream_st* sj_stream_t;
+
+/* Status codes. The adapter maps SJ_ERR_OOM to rmm::out_of_memory so that Sirius's
+ * oom_reschedule path still fires (src/pipeline/gpu_pipeline_task.cpp:386-437); everything else
+ * becomes std::runtime_error, as the operator's own misuse errors are
+ * (src/op/sirius_physical_hash_join.cpp:1548-1564). */
+typedef enum sj_status {
+  SJ_OK             = 0,
+  SJ_ERR_OOM        = 1, /* the allocator returned NULL */
+  SJ_ERR_TABLE_FULL = 2, /* a bounded insert ran out of slots */
+  SJ_ERR_INVALID    = 3, /* bad argument (types, sizes, null pointers, alignment) */
+  SJ_ERR_DEVICE     = 4, /* a CUDA runtime call failed */
+  SJ_ERR_TIMEOUT    = 5, /* a bounded wait gave up */
+  SJ_ERR_CAPACITY   = 6, /* more output rows than the capacity the caller gave */
+  SJ_ERR_BUSY       = 7  /* admission refused (memory budget / queue full) */
+} sj_status;
+
+/* Fixed-width column types. Keys must be SJ_INT32 or SJ_INT64 (cuDF INT32/INT64 and the types
+ * Sirius stores in them, e.g. DATE / TIMESTAMP); payloads may be any of these. */
+typedef enum sj_type {
+  SJ_TYPE_INVALID = 0,
+  SJ_INT8         = 1,
+  SJ_INT16        = 2,
+  SJ_INT32        = 3,
+  SJ_INT64        = 4,
+  SJ_FLOAT32      = 5,
+  SJ_FLOAT64      = 6,
+  SJ_BOOL8        = 7,
+  SJ_UINT32       = 8,
+  SJ_UINT64       = 9
+} sj_type;
+
+/* A read-only column view (cudf::column_view: data<T>() , null_mask(), offset(), size()). */
+typedef struct sj_column {
+  const void* data;         /* row 0 of the column (head + offset already applied) */
+  const uint32_t* validity; /* NULL = all rows valid */
+  int64_t validity_offset;  /* bit index of row 0 inside validity */
+  int64_t num_rows;
+  int32_t type;             /* sj_type */
+  int32_t reserved;
+} sj_column;
+
+/* A writable output column: num_rows is given by the call's capacity. */
+typedef struct sj_mut_column {
+  void* data;
+  uint32_t* validity; /* required iff the matching input payload column has validity */
+  int32_t type;       /* sj_type, must equal the input payload type */
+  int32_t reserved;
+} sj_mut_column;
+
+/* Device memory comes from the caller (Sirius: the cuCascade reservation-aware RMM resource the
+ * task attached to its stream, src/pipeline/gpu_pipeline_task.cpp:523-525). Passing NULL where
+ * an sj_alloc* is accepted uses cudaMallocAsync / cudaFreeAsync on the call's stream. */
+typedef struct sj_alloc {
+  void* ctx;
+  void* (*alloc)(void* ctx, size_t bytes, sj_stream_t stream);
+  void (*free)(void* ctx, void* ptr, size_t bytes, sj_stream_t stream);
+} sj_alloc;
+
+/* NULL semantics of the key comparison: cudf::null_equality as the operator caches it in
+ * compare_nulls_ (src/op/sirius_physical_hash_join.cpp:252-264). UNEQUAL: NULL never matches.
+ * EQUAL: NULL matches NULL (every key IS NOT DISTINCT FROM). */
+typedef enum sj_null_equality { SJ_NULLS_UNEQUAL = 0, SJ_NULLS_EQUAL = 1 } sj_null_equality;
+
+/* Table layout. AUTO builds a DISTINCT table when the valid build keys are unique and a GROUPED
+ * table otherwise; GROUPED forces the grouped layout. */
+typedef enum sj_layout {
+  SJ_LAYOUT_AUTO     = 0,
+  SJ_LAYOUT_DISTINCT = 1, /* one slot per build row, keys unique (cudf::distinct_hash_join) */
+  SJ_LAYOUT_GROUPED  = 2  /* one slot per distinct key + a row-id range (cudf::hash_join multiset) */
+} sj_layout;
+
+/* Slot encoding chosen at build time from the key range. */
+typedef enum sj_slot_kind {
+  SJ_SLOT_PACKED64 = 0, /* (key - key_min) << rid_bits | row id, inserted by 64-bit atomicCAS */
+  SJ_SLOT_WIDE128  = 1  /* {int64 key, row id} pair, inserted by 128-bit atomicCAS */
+} sj_slot_kind;
+
+/* Tunables. Zero-initialised fields take defaults (sj_default_params fills them in). */
+typedef struct sj_join_params {
+  int32_t layout;           /* sj_layout */
+  int32_t null_equality;    /* sj_null_equality */
+  float load_factor;        /* slots in use / slots; default 0.5 (the distinct_hash_join value) */
+  int32_t block_size;       /* threads per CTA for probe kernels; default 256 */
+  int32_t group_width;      /* probe group width 1,2,4,8,16,32 lanes per key; default 1 */
+  int32_t partition_bits;   /* radix bits of the partitioned variant; 0 = not partitioned */
+  int32_t force_wide;       /* 1 = use SJ_SLOT_WIDE128 even when the packed encoding fits */
+  int32_t ctas_per_sm;      /* grid = ctas_per_sm * SM count for grid-stride kernels; default 4 */
+  int32_t reserved[8];
+} sj_join_params;
+
+typedef struct sj_table sj_table;
+
+typedef struct sj_table_info {
+  int64_t build_rows;      /* rows of the build key column */
+  int64_t valid_rows;      /* rows with a non-NULL key */
+  int64_t null_rows;       /* rows with a NULL key */
+  int64_t distinct_keys;   /* distinct non-NULL keys */
+  int64_t num_slots;       /* slots in the open-addressing table */
+  int64_t device_bytes;    /* bytes held on the device by the table */
+  int64_t key_min;         /* smallest valid key (0 if none) */
+  int64_t key_max;         /* largest valid key (-1 if none) */
+  int32_t layout;          /* sj_layout actually built (DISTINCT or GROUPED) */
+  int32_t slot_kind;       /* sj_slot_kind */
+  int32_t rid_bits;        /* row-id bits of a packed slot */
+  int32_t key_type;        /* sj_type of the key */
+  int32_t partition_bits;  /* radix bits (0 = not partitioned) */
+  int32_t max_group;       /* largest number of build rows sharing one key */
+} sj_table_info;
+
+/* ---------------------------------------------------------------------------------------------
+ * Core join: build, probe, gather.
+ * ------------------------------------------------------------------------------------------- */
+
+/* Fill *params with defaults. */
+SJ_EXPORT void sj_default_params(sj_join_params* params);
+
+/* Build a hash table over the build keys (replaces the cudf::hash_join / distinct_hash_join
+ * constructors, src/op/sirius_physical_hash_join.cpp:1614-1620). Row ids in the table are the
+ * build column's row indices. Only num_keys == 1 is accepted. Rows with a NULL key are not
+ * inserted under SJ_NULLS_UNEQUAL. The key column is only read during the call; the caller keeps
+ * the build batch alive for the gather, as the operator does (:1593).
+ * Synchronizes `stream` (once to size the table from the key range, once to choose the layout);
+ * the reference synchronizes after the build as well (:1622). */
+SJ_EXPORT sj_status sj_build(const sj_column* keys, int32_t num_keys, const sj_join_params* params,
+                             const sj_alloc* alloc, sj_stream_t stream, sj_table** out);
+
+/* Free the table's device memory, stream-ordered on `stream` (on_finalize_operator frees each
+ * slot's table on its device, src/op/sirius_physical_hash_join.cpp:2084-2097). */
+SJ_EXPORT sj_status sj_table_destroy(sj_table* table, sj_stream_t stream);
+
+SJ_EXPORT sj_status sj_table_get_info(const sj_table* table, sj_table_info* info);
+
+/* Count the INNER matches of the probe keys (the size pass cuDF runs before retrieval for the
+ * multiset inner_join). Writes the count to *d_count (device int64). Stream-ordered. */
+SJ_EXPORT sj_status sj_probe_count(const sj_table* table, const sj_column* probe_keys,
+                                   int32_t num_keys, const sj_alloc* alloc, sj_stream_t stream,
+                                   int64_t* d_count);
+
+/* INNER probe fused with the payload gather (replaces inner_join + gather_join_output,
+ * src/op/sirius_physical_hash_join.cpp:1671, :1688, :1299-1359).
+ * For every (probe row i, build row j) with equal keys it writes, at one output position p:
+ *   out_probe_rid[p] = i, out_build_rid[p] = j   (either pointer may be NULL: not written)
+ *   out_probe_payload[c][p] = probe_payload[c][i]
+ *   out_build_payload[c][p] = build_payload[c][j]
+ * and validity bits copied from the payload columns (NULLIFY is not needed for INNER).
+ * *d_count (device int64) receives the total number of matches M; only positions p < capacity
+ * are written, so the call succeeded iff M <= capacity (read *d_count after the stream).
+ * A DISTINCT table never has M > probe rows. Output order is unspecified, as cuDF's is.
+ * Stream-ordered; scratch for GROUPED tables comes from `alloc`. */
+SJ_EXPORT sj_status sj_probe_gather(const sj_table* table, const sj_column* probe_keys,
+                                    int32_t num_keys, const sj_column* probe_payload,
+                                    int32_t num_probe_payload, const sj_column* build_payload,
+                                    int32_t num_build_payload, int32_t* out_probe_rid,
+                                    int32_t* out_build_rid, const sj_mut_column* out_probe_payload,
+                                    const sj_mut_column* out_build_payload, int64_t capacity,
+                                    const sj_alloc* alloc, sj_stream_t stream, int64_t* d_count);
+
+/* One-shot INNER join (STANDARD mode: cudf::inner_join(left_keys, right_keys, compare_nulls(),
+ * stream), src/op/sirius_physical_hash_join.cpp:1872, followed by gather_join_output): builds a
+ * throwaway table on build_keys, probes it with probe_keys and gathers. Same output contract as
+ * sj_probe_gather. Synchronizes `stream` like sj_build. */
+SJ_EXPORT sj_status sj_inner_join(const sj_column* build_keys, const sj_column* probe_keys,
+                                  int32_t num_keys, const sj_column* probe_payload,
+                                  int32_t num_probe_payload, const sj_column* build_payload,
+                                  int32_t num_build_payload, int32_t* out_probe_rid,
+                                  int32_t* out_build_rid, const sj_mut_column* out_probe_payload,
+                                  const sj_mut_column* out_build_payload, int64_t capacity,
+                                  const sj_join_params* params, const sj_alloc* alloc,
+                                  sj_stream_t stream, int64_t* d_count);
+
+/* ---------------------------------------------------------------------------------------------
+ * Diagnostics.
+ * ------------------------------------------------------------------------------------------- */
+
+SJ_EXPORT const char* sj_status_string(sj_status status);
+
+/* Message of the last failing call on this thread ("" if none). */
+SJ_EXPORT const char* sj_last_error(void);
+
+/* ABI version: major * 10000 + minor * 100 + patch. */
+SJ_EXPORT int32_t sj_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SJ_JOIN_H */

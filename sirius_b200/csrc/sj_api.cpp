@@ -1,0 +1,246 @@
+// C ABI entry points of the join (declared in include/sj/sj_join.h). Each one validates its
+// arguments, converts C++ failures into sj_status + a per-thread message, and never throws.
+#include <cuda_runtime.h>
+
+#include <cstring>
+#include <mutex>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "sj_internal.h"
+
+namespace sj {
+
+static thread_local std::string g_last_error;
+
+sj_status set_error(sj_status st, const std::string& msg) {
+  g_last_error = msg;
+  return st;
+}
+void clear_error() { g_last_error.clear(); }
+
+Allocator::Allocator(const sj_alloc* user) {
+  if (user && user->alloc && user->free) {
+    a = *user;
+    use_default = false;
+  }
+}
+
+sj_status Allocator::allocate(void** p, size_t bytes, cudaStream_t s) const {
+  *p = nullptr;
+  if (bytes == 0) bytes = 16;
+  if (use_default) {
+    cudaError_t e = cudaMallocAsync(p, bytes, s);
+    if (e != cudaSuccess || *p == nullptr) {
+      cudaGetLastError();  // clear the non-sticky allocation error
+      *p = nullptr;
+      return set_error(SJ_ERR_OOM, "cudaMallocAsync of " + std::to_string(bytes) + " bytes failed");
+    }
+    return SJ_OK;
+  }
+  *p = a.alloc(a.ctx, bytes, reinterpret_cast<sj_stream_t>(s));
+  if (*p == nullptr) return set_error(SJ_ERR_OOM, "allocator callback returned NULL for " + std::to_string(bytes) + " bytes");
+  return SJ_OK;
+}
+
+void Allocator::release(void* p, size_t bytes, cudaStream_t s) const {
+  if (!p) return;
+  if (bytes == 0) bytes = 16;
+  if (use_default) cudaFreeAsync(p, s);
+  else a.free(a.ctx, p, bytes, reinterpret_cast<sj_stream_t>(s));
+}
+
+int sm_count(int device) {
+  static std::mutex mu;
+  static std::vector<int> cache;
+  std::lock_guard<std::mutex> lk(mu);
+  if (device < 0) device = 0;
+  if ((int)cache.size() <= device) cache.resize(device + 1, 0);
+  if (cache[device] == 0) {
+    int v = 0;
+    if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, device) != cudaSuccess || v <= 0) v = 148;
+    cache[device] = v;
+  }
+  return cache[device];
+}
+
+int type_width(int32_t t) {
+  switch (t) {
+    case SJ_INT8:
+    case SJ_BOOL8: return 1;
+    case SJ_INT16: return 2;
+    case SJ_INT32:
+    case SJ_FLOAT32:
+    case SJ_UINT32: return 4;
+    case SJ_INT64:
+    case SJ_FLOAT64:
+    case SJ_UINT64: return 8;
+    default: return 0;
+  }
+}
+
+sj_status validate_column(const sj_column* c, const char* what, bool key) {
+  if (!c) return set_error(SJ_ERR_INVALID, std::string(what) + " column is NULL");
+  if (c->num_rows < 0) return set_error(SJ_ERR_INVALID, std::string(what) + " column has negative num_rows");
+  if (key) {
+    if (c->type != SJ_INT32 && c->type != SJ_INT64)
+      return set_error(SJ_ERR_INVALID, std::string(what) + " column must be INT32 or INT64");
+  } else if (type_width(c->type) == 0) {
+    return set_error(SJ_ERR_INVALID, std::string(what) + " column has an unknown type");
+  }
+  if (c->num_rows > 0 && c->data == nullptr)
+    return set_error(SJ_ERR_INVALID, std::string(what) + " column data is NULL");
+  if (c->validity_offset < 0) return set_error(SJ_ERR_INVALID, std::string(what) + " validity_offset < 0");
+  const uintptr_t align = (uintptr_t)type_width(c->type);
+  if (c->data && ((uintptr_t)c->data % align) != 0)
+    return set_error(SJ_ERR_INVALID, std::string(what) + " column data is not aligned to its element size");
+  return SJ_OK;
+}
+
+static sj_join_params resolve(const sj_join_params* p) {
+  sj_join_params r;
+  sj_default_params(&r);
+  if (!p) return r;
+  r.layout = p->layout;
+  r.null_equality = p->null_equality;
+  if (p->load_factor > 0.0f) r.load_factor = p->load_factor;
+  if (p->block_size > 0) r.block_size = p->block_size;
+  if (p->group_width > 0) r.group_width = p->group_width;
+  r.partition_bits = p->partition_bits;
+  r.force_wide = p->force_wide;
+  if (p->ctas_per_sm > 0) r.ctas_per_sm = p->ctas_per_sm;
+  return r;
+}
+
+}  // namespace sj
+
+using namespace sj;
+
+extern "C" {
+
+SJ_EXPORT void sj_default_params(sj_join_params* p) {
+  if (!p) return;
+  std::memset(p, 0, sizeof(*p));
+  p->layout = SJ_LAYOUT_AUTO;
+  p->null_equality = SJ_NULLS_UNEQUAL;
+  p->load_factor = 0.5f;
+  p->block_size = 256;
+  p->group_width = 1;
+  p->partition_bits = 0;
+  p->force_wide = 0;
+  p->ctas_per_sm = 4;
+}
+
+SJ_EXPORT sj_status sj_build(const sj_column* keys, int32_t num_keys, const sj_join_params* params,
+                             const sj_alloc* alloc, sj_stream_t stream, sj_table** out) {
+  clear_error();
+  if (!out) return set_error(SJ_ERR_INVALID, "out is NULL");
+  *out = nullptr;
+  if (num_keys != 1) return set_error(SJ_ERR_INVALID, "exactly one key column is supported");
+  if (!keys) return set_error(SJ_ERR_INVALID, "keys is NULL");
+  try {
+    const sj_join_params p = resolve(params);
+    return build_table(keys[0], p, Allocator(alloc), reinterpret_cast<cudaStream_t>(stream), out);
+  } catch (const std::bad_alloc&) {
+    return set_error(SJ_ERR_OOM, "host allocation failed");
+  } catch (const std::exception& e) {
+    return set_error(SJ_ERR_DEVICE, e.what());
+  }
+}
+
+SJ_EXPORT sj_status sj_table_destroy(sj_table* table, sj_stream_t stream) {
+  clear_error();
+  return destroy_table(table, reinterpret_cast<cudaStream_t>(stream));
+}
+
+SJ_EXPORT sj_status sj_table_get_info(const sj_table* t, sj_table_info* info) {
+  clear_error();
+  if (!t || !info) return set_error(SJ_ERR_INVALID, "table or info is NULL");
+  std::memset(info, 0, sizeof(*info));
+  info->build_rows = t->build_rows;
+  info->valid_rows = t->valid_rows;
+  info->null_rows = t->null_rows;
+  info->distinct_keys = t->distinct;
+  info->num_slots = t->num_slots();
+  info->device_bytes = (int64_t)(t->slots_bytes + t->grp_off_bytes + t->grp_rid_bytes);
+  info->key_min = t->valid_rows ? t->kmin : 0;
+  info->key_max = t->valid_rows ? t->kmax : -1;
+  info->layout = t->layout;
+  info->slot_kind = t->slot_kind;
+  info->rid_bits = t->rid_bits;
+  info->key_type = t->key_type;
+  info->partition_bits = t->pbits;
+  info->max_group = t->max_group;
+  return SJ_OK;
+}
+
+SJ_EXPORT sj_status sj_probe_count(const sj_table* table, const sj_column* probe_keys, int32_t num_keys,
+                                   const sj_alloc* alloc, sj_stream_t stream, int64_t* d_count) {
+  clear_error();
+  if (!table || !probe_keys || !d_count) return set_error(SJ_ERR_INVALID, "table, probe_keys and d_count are required");
+  if (num_keys != 1) return set_error(SJ_ERR_INVALID, "exactly one key column is supported");
+  try {
+    return probe_count(table, probe_keys[0], Allocator(alloc), reinterpret_cast<cudaStream_t>(stream), d_count);
+  } catch (const std::exception& e) {
+    return set_error(SJ_ERR_DEVICE, e.what());
+  }
+}
+
+SJ_EXPORT sj_status sj_probe_gather(const sj_table* table, const sj_column* probe_keys, int32_t num_keys,
+                                    const sj_column* probe_payload, int32_t num_probe_payload,
+                                    const sj_column* build_payload, int32_t num_build_payload,
+                                    int32_t* out_probe_rid, int32_t* out_build_rid,
+                                    const sj_mut_column* out_probe_payload, const sj_mut_column* out_build_payload,
+                                    int64_t capacity, const sj_alloc* alloc, sj_stream_t stream, int64_t* d_count) {
+  clear_error();
+  if (!table || !probe_keys || !d_count) return set_error(SJ_ERR_INVALID, "table, probe_keys and d_count are required");
+  if (num_keys != 1) return set_error(SJ_ERR_INVALID, "exactly one key column is supported");
+  GatherSpec g{probe_payload, num_probe_payload, build_payload, num_build_payload, out_probe_rid,
+               out_build_rid, out_probe_payload, out_build_payload, capacity};
+  try {
+    return probe_gather(table, probe_keys[0], g, Allocator(alloc), reinterpret_cast<cudaStream_t>(stream), d_count);
+  } catch (const std::exception& e) {
+    return set_error(SJ_ERR_DEVICE, e.what());
+  }
+}
+
+SJ_EXPORT sj_status sj_inner_join(const sj_column* build_keys, const sj_column* probe_keys, int32_t num_keys,
+                                  const sj_column* probe_payload, int32_t num_probe_payload,
+                                  const sj_column* build_payload, int32_t num_build_payload, int32_t* out_probe_rid,
+                                  int32_t* out_build_rid, const sj_mut_column* out_probe_payload,
+                                  const sj_mut_column* out_build_payload, int64_t capacity,
+                                  const sj_join_params* params, const sj_alloc* alloc, sj_stream_t stream,
+                                  int64_t* d_count) {
+  clear_error();
+  sj_table* t = nullptr;
+  sj_status st = sj_build(build_keys, num_keys, params, alloc, stream, &t);
+  if (st != SJ_OK) return st;
+  st = sj_probe_gather(t, probe_keys, num_keys, probe_payload, num_probe_payload, build_payload,
+                       num_build_payload, out_probe_rid, out_build_rid, out_probe_payload, out_build_payload,
+                       capacity, alloc, stream, d_count);
+  const std::string msg = sj_last_error();
+  destroy_table(t, reinterpret_cast<cudaStream_t>(stream));
+  if (st != SJ_OK) set_error(st, msg);
+  return st;
+}
+
+SJ_EXPORT const char* sj_status_string(sj_status s) {
+  switch (s) {
+    case SJ_OK: return "SJ_OK";
+    case SJ_ERR_OOM: return "SJ_ERR_OOM";
+    case SJ_ERR_TABLE_FULL: return "SJ_ERR_TABLE_FULL";
+    case SJ_ERR_INVALID: return "SJ_ERR_INVALID";
+    case SJ_ERR_DEVICE: return "SJ_ERR_DEVICE";
+    case SJ_ERR_TIMEOUT: return "SJ_ERR_TIMEOUT";
+    case SJ_ERR_CAPACITY: return "SJ_ERR_CAPACITY";
+    case SJ_ERR_BUSY: return "SJ_ERR_BUSY";
+  }
+  return "SJ_ERR_UNKNOWN";
+}
+
+SJ_EXPORT const char* sj_last_error(void) { return g_last_error.c_str(); }
+
+SJ_EXPORT int32_t sj_version(void) { return 100; }
+
+}  // extern "C"

@@ -1,0 +1,501 @@
+// Hash-table build for the sm_100a equi-join (replaces the cudf::hash_join /
+// cudf::distinct_hash_join constructors called at src/op/sirius_physical_hash_join.cpp:1614-1620).
+//
+// Passes (all stream-ordered on the caller's stream):
+//   1. stats    min / max of the valid keys, valid and NULL row counts (one read of the keys).
+//               The host reads them (sync #1) to pick the slot encoding and the table size.
+//   2. insert   insert-or-find: each valid row CASes ((key-kmin) << rid_bits | row) into the first
+//               EMPTY slot of its probe sequence unless its key is already present, in which case
+//               it only counts a duplicate. The host reads the duplicate count (sync #2).
+//   3. grouped  only when duplicates exist (or GROUPED is forced, or NULLs are equal):
+//               count rows per slot (warp-aggregated with __match_any_sync), exclusive scan of the
+//               counts into per-slot offsets, scatter row ids into one array ordered by group.
+//               Duplicated keys then cost one slot each and a probe expands a whole group as a
+//               contiguous row-id range, so a key with 10^6 copies is no longer a 10^6-slot cluster.
+// A DISTINCT table is the result of pass 2 alone: one slot per build row (the unique-key case of
+// distinct_hash_join, load factor 0.5 by default as at :1615).
+#include <algorithm>
+#include <climits>
+#include <cstring>
+
+#include "sj_device.cuh"
+#include "sj_internal.h"
+#include "sj_scan.cuh"
+
+namespace sj {
+
+struct BuildStats {
+  long long kmin;
+  long long kmax;
+  unsigned long long n_valid;
+  unsigned long long n_null;
+  unsigned long long n_dup;
+  unsigned int full;
+  unsigned int max_group;
+};
+
+__global__ void stats_init_kernel(BuildStats* st) {
+  st->kmin = LLONG_MAX;
+  st->kmax = LLONG_MIN;
+  st->n_valid = 0;
+  st->n_null = 0;
+  st->n_dup = 0;
+  st->full = 0;
+  st->max_group = 0;
+}
+
+template <typename K>
+__global__ void __launch_bounds__(256) stats_kernel(const K* __restrict__ keys, const uint32_t* kv,
+                                                    int64_t kvoff, int64_t n, BuildStats* st) {
+  long long mn = LLONG_MAX, mx = LLONG_MIN;
+  unsigned long long nv = 0, nn = 0;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    if (bit_valid(kv, kvoff, i)) {
+      const long long k = (long long)keys[i];
+      mn = k < mn ? k : mn;
+      mx = k > mx ? k : mx;
+      ++nv;
+    } else {
+      ++nn;
+    }
+  }
+#pragma unroll
+  for (int d = 16; d > 0; d >>= 1) {
+    long long a = __shfl_down_sync(kFullMask, mn, d);
+    long long b = __shfl_down_sync(kFullMask, mx, d);
+    mn = a < mn ? a : mn;
+    mx = b > mx ? b : mx;
+    nv += __shfl_down_sync(kFullMask, nv, d);
+    nn += __shfl_down_sync(kFullMask, nn, d);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    if (nv) {
+      atomicMin(&st->kmin, mn);
+      atomicMax(&st->kmax, mx);
+      atomicAdd(&st->n_valid, nv);
+    }
+    if (nn) atomicAdd(&st->n_null, nn);
+  }
+}
+
+// Insert-or-find one key. Returns 0 = inserted, 1 = key already present, 2 = segment full.
+template <bool WIDE>
+__device__ __forceinline__ int insert_or_find(const TableDev& t, uint64_t kb, uint64_t kn, int32_t row,
+                                              uint32_t* slot_out) {
+  using Ops = SlotOps<WIDE>;
+  void* slots = const_cast<void*>(t.slots);
+  uint32_t b = home_bucket(t, kb);
+  const uint64_t packed = (kn << t.rbits) | (uint64_t)(uint32_t)row;
+  for (uint32_t step = 0; step <= t.segmask; ++step) {
+    Bucket bk = load_bucket<false>(slots, b);
+#pragma unroll
+    for (int q = 0; q < Ops::kSlots; ++q) {
+      if (Ops::empty(bk, q)) {
+        if (!WIDE) {
+          unsigned long long* p = reinterpret_cast<unsigned long long*>(slots) + (size_t)b * 4 + q;
+          const unsigned long long old = atomicCAS(p, kEmpty, packed);
+          if (old == kEmpty) {
+            *slot_out = b * Ops::kSlots + q;
+            return 0;
+          }
+          bk.a[q] = old;
+        } else {
+          uint64_t* p = reinterpret_cast<uint64_t*>(slots) + (size_t)b * 4 + 2 * q;
+          uint64_t olo, ohi;
+          cas128(p, kEmpty, kEmpty, kb, (uint64_t)(uint32_t)row, olo, ohi);
+          if (ohi == kEmpty) {
+            *slot_out = b * Ops::kSlots + q;
+            return 0;
+          }
+          bk.a[2 * q] = olo;
+          bk.a[2 * q + 1] = ohi;
+        }
+      }
+      if (Ops::match(bk, q, kn, kb, t.rbits)) {
+        *slot_out = b * Ops::kSlots + q;
+        return 1;
+      }
+    }
+    b = next_bucket(b, t.segmask);
+  }
+  return 2;
+}
+
+// Find the slot of a key known to be in the table (grouped passes). UINT32_MAX if absent.
+template <bool WIDE>
+__device__ __forceinline__ uint32_t find_slot(const TableDev& t, uint64_t kb, uint64_t kn) {
+  using Ops = SlotOps<WIDE>;
+  uint32_t b = home_bucket(t, kb);
+  for (uint32_t step = 0; step <= t.segmask; ++step) {
+    const Bucket bk = load_bucket<true>(t.slots, b);
+    bool has_empty = false;
+#pragma unroll
+    for (int q = 0; q < Ops::kSlots; ++q) {
+      if (Ops::match(bk, q, kn, kb, t.rbits)) return b * Ops::kSlots + q;
+      has_empty |= Ops::empty(bk, q);
+    }
+    if (has_empty) break;
+    b = next_bucket(b, t.segmask);
+  }
+  return 0xffffffffu;
+}
+
+template <typename K, bool WIDE>
+__global__ void __launch_bounds__(256) insert_kernel(TableDev t, const K* __restrict__ keys,
+                                                     const uint32_t* kv, int64_t kvoff, int64_t n,
+                                                     BuildStats* st) {
+  const int lane = threadIdx.x & 31;
+  for (int64_t i0 = (int64_t)blockIdx.x * blockDim.x; i0 < n; i0 += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t i = i0 + threadIdx.x;
+    int r = -1;
+    if (i < n && bit_valid(kv, kvoff, i)) {
+      const K k = keys[i];
+      const uint64_t kb = key_u64<K>(k);
+      const uint64_t kn = (uint64_t)(long long)k - (uint64_t)t.kmin;
+      uint32_t s;
+      r = insert_or_find<WIDE>(t, kb, kn, (int32_t)i, &s);
+    }
+    const unsigned dup = __ballot_sync(kFullMask, r == 1);
+    const unsigned full = __ballot_sync(kFullMask, r == 2);
+    if (lane == 0) {
+      if (dup) atomicAdd(&st->n_dup, (unsigned long long)__popc(dup));
+      if (full) atomicOr(&st->full, 1u);
+    }
+  }
+}
+
+// Copy every live slot of `src` into `dst` (a smaller table): the grouped build shrinks the
+// table to its distinct keys so that the probe's random reads hit a table sized by distinct keys.
+template <bool WIDE>
+__global__ void __launch_bounds__(256) reinsert_kernel(TableDev src, uint64_t src_buckets, TableDev dst,
+                                                       BuildStats* st) {
+  using Ops = SlotOps<WIDE>;
+  for (uint64_t b = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; b < src_buckets;
+       b += (uint64_t)gridDim.x * blockDim.x) {
+    const Bucket bk = load_bucket<true>(src.slots, (uint32_t)b);
+#pragma unroll
+    for (int q = 0; q < Ops::kSlots; ++q) {
+      if (Ops::empty(bk, q)) continue;
+      uint64_t kb, kn;
+      int32_t row;
+      if (!WIDE) {
+        kn = bk.a[q] >> src.rbits;
+        kb = kn + (uint64_t)src.kmin;
+        row = (int32_t)(bk.a[q] & ((1ull << src.rbits) - 1));
+      } else {
+        kb = bk.a[2 * q];
+        kn = kb - (uint64_t)src.kmin;
+        row = (int32_t)bk.a[2 * q + 1];
+      }
+      uint32_t s;
+      if (insert_or_find<WIDE>(dst, kb, kn, row, &s) == 2) atomicOr(&st->full, 1u);
+    }
+  }
+}
+
+// Grouped pass A: rows per slot. NULL-key rows count into the NULL group when NULLs are equal.
+template <typename K, bool WIDE>
+__global__ void __launch_bounds__(256) group_count_kernel(TableDev t, const K* __restrict__ keys,
+                                                          const uint32_t* kv, int64_t kvoff, int64_t n,
+                                                          int32_t* cnt, BuildStats* st) {
+  const int lane = threadIdx.x & 31;
+  unsigned int local_max = 0;
+  for (int64_t i0 = (int64_t)blockIdx.x * blockDim.x; i0 < n; i0 += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t i = i0 + threadIdx.x;
+    int64_t s = -1;
+    if (i < n) {
+      if (bit_valid(kv, kvoff, i)) {
+        const K k = keys[i];
+        const uint64_t kb = key_u64<K>(k);
+        const uint64_t kn = (uint64_t)(long long)k - (uint64_t)t.kmin;
+        const uint32_t f = find_slot<WIDE>(t, kb, kn);
+        if (f != 0xffffffffu) s = f;
+      } else if (t.null_group >= 0) {
+        s = t.null_group;
+      }
+    }
+    const unsigned peers = __match_any_sync(kFullMask, (unsigned long long)s);
+    const int leader = __ffs(peers) - 1;
+    if (s >= 0 && lane == leader) {
+      const int add = __popc(peers);
+      const int now = atomicAdd(cnt + s, add) + add;
+      local_max = (unsigned)now > local_max ? (unsigned)now : local_max;
+    }
+  }
+#pragma unroll
+  for (int d = 16; d > 0; d >>= 1) {
+    unsigned o = __shfl_down_sync(kFullMask, local_max, d);
+    local_max = o > local_max ? o : local_max;
+  }
+  if (lane == 0 && local_max) atomicMax(&st->max_group, local_max);
+}
+
+// Grouped pass B: scatter row ids into their group's range (cursor starts at zero).
+template <typename K, bool WIDE>
+__global__ void __launch_bounds__(256) group_scatter_kernel(TableDev t, const K* __restrict__ keys,
+                                                            const uint32_t* kv, int64_t kvoff, int64_t n,
+                                                            const int32_t* __restrict__ off,
+                                                            int32_t* cursor, int32_t* grp_rid) {
+  const int lane = threadIdx.x & 31;
+  for (int64_t i0 = (int64_t)blockIdx.x * blockDim.x; i0 < n; i0 += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t i = i0 + threadIdx.x;
+    int64_t s = -1;
+    if (i < n) {
+      if (bit_valid(kv, kvoff, i)) {
+        const K k = keys[i];
+        const uint64_t kb = key_u64<K>(k);
+        const uint64_t kn = (uint64_t)(long long)k - (uint64_t)t.kmin;
+        const uint32_t f = find_slot<WIDE>(t, kb, kn);
+        if (f != 0xffffffffu) s = f;
+      } else if (t.null_group >= 0) {
+        s = t.null_group;
+      }
+    }
+    const unsigned peers = __match_any_sync(kFullMask, (unsigned long long)s);
+    const int leader = __ffs(peers) - 1;
+    int base = 0;
+    if (s >= 0 && lane == leader) base = atomicAdd(cursor + s, __popc(peers));
+    base = __shfl_sync(kFullMask, base, leader);
+    if (s >= 0) {
+      const int rank = __popc(peers & ((1u << lane) - 1));
+      grp_rid[off[s] + base + rank] = (int32_t)i;
+    }
+  }
+}
+
+// ------------------------------------------------------------------------------------------------
+// host side
+// ------------------------------------------------------------------------------------------------
+
+static int bit_width_u64(uint64_t v) { return v ? 64 - __builtin_clzll(v) : 0; }
+
+static TableDev make_dev(const sj_table* t) {
+  TableDev d{};
+  d.slots = t->slots;
+  d.grp_off = t->grp_off;
+  d.grp_rid = t->grp_rid;
+  d.kmin = t->kmin;
+  d.kmax = t->kmax;
+  d.log2_nb = (uint32_t)t->log2_nb;
+  d.segmask = (uint32_t)((1ull << t->seg_log2) - 1);
+  d.rbits = (uint32_t)t->rid_bits;
+  d.null_group = -1;
+  if (t->layout == SJ_LAYOUT_GROUPED && t->null_eq == SJ_NULLS_EQUAL && t->null_rows > 0)
+    d.null_group = (int32_t)t->num_slots();
+  return d;
+}
+
+TableDev table_dev(const sj_table* t) { return make_dev(t); }
+
+static int grid_for(int device, const sj_join_params& p, int64_t work_items, int per_cta) {
+  const int64_t need = (work_items + per_cta - 1) / per_cta;
+  const int64_t cap = (int64_t)sm_count(device) * std::max(1, p.ctas_per_sm) * 2;
+  return (int)std::max<int64_t>(1, std::min(need, cap));
+}
+
+template <typename K>
+static void launch_stats(const sj_column& c, int grid, BuildStats* st, cudaStream_t s) {
+  stats_kernel<K><<<grid, 256, 0, s>>>(static_cast<const K*>(c.data), c.validity, c.validity_offset,
+                                       c.num_rows, st);
+}
+
+template <typename K, bool WIDE>
+static void launch_insert(const TableDev& d, const sj_column& c, int grid, BuildStats* st, cudaStream_t s) {
+  insert_kernel<K, WIDE><<<grid, 256, 0, s>>>(d, static_cast<const K*>(c.data), c.validity,
+                                              c.validity_offset, c.num_rows, st);
+}
+
+template <typename K, bool WIDE>
+static void launch_group(const TableDev& d, const sj_column& c, int grid, int32_t* cnt, int32_t* off,
+                         int32_t* grp_rid, bool scatter, BuildStats* st, cudaStream_t s) {
+  if (!scatter)
+    group_count_kernel<K, WIDE><<<grid, 256, 0, s>>>(d, static_cast<const K*>(c.data), c.validity,
+                                                     c.validity_offset, c.num_rows, cnt, st);
+  else
+    group_scatter_kernel<K, WIDE><<<grid, 256, 0, s>>>(d, static_cast<const K*>(c.data), c.validity,
+                                                       c.validity_offset, c.num_rows, off, cnt, grp_rid);
+}
+
+static sj_status alloc_slots(sj_table* t, int log2_nb, cudaStream_t s) {
+  t->log2_nb = log2_nb;
+  t->seg_log2 = log2_nb - std::min(t->pbits, log2_nb);
+  t->slots_bytes = ((size_t)1 << log2_nb) * kBucketBytes;
+  SJ_TRY(t->alloc.allocate(&t->slots, t->slots_bytes, s));
+  SJ_CUDA_TRY(cudaMemsetAsync(t->slots, 0xff, t->slots_bytes, s));
+  return SJ_OK;
+}
+
+static int log2_buckets_for(int64_t keys, double lf, int slots_per_bucket) {
+  const double slots = std::max<double>(1.0, (double)std::max<int64_t>(keys, 1) / lf);
+  const int64_t buckets = (int64_t)std::ceil(slots / slots_per_bucket);
+  int l = 0;
+  while ((1ll << l) < buckets) ++l;
+  return l;
+}
+
+sj_status build_table(const sj_column& keys, const sj_join_params& p, const Allocator& alloc,
+                      cudaStream_t stream, sj_table** out) {
+  SJ_TRY(validate_column(&keys, "build key", true));
+  if (keys.num_rows > INT32_MAX)
+    return set_error(SJ_ERR_INVALID, "build side exceeds the int32 row-id range");
+  if (!(p.load_factor > 0.0f && p.load_factor < 1.0f))
+    return set_error(SJ_ERR_INVALID, "load_factor must be in (0, 1)");
+  if (p.layout < SJ_LAYOUT_AUTO || p.layout > SJ_LAYOUT_GROUPED)
+    return set_error(SJ_ERR_INVALID, "unknown layout");
+  if (p.partition_bits < 0 || p.partition_bits > 16)
+    return set_error(SJ_ERR_INVALID, "partition_bits must be in [0, 16]");
+
+  sj_table* t = new sj_table();
+  t->alloc = alloc;
+  cudaGetDevice(&t->device);
+  t->key_type = keys.type;
+  t->null_eq = p.null_equality;
+  t->params = p;
+  t->pbits = p.partition_bits;
+  t->build_rows = keys.num_rows;
+  auto fail = [&](sj_status st) {
+    destroy_table(t, stream);
+    return st;
+  };
+
+  Scratch st_buf;
+  if (sj_status e = st_buf.get(alloc, sizeof(BuildStats), stream)) return fail(e);
+  BuildStats* st = st_buf.as<BuildStats>();
+  stats_init_kernel<<<1, 1, 0, stream>>>(st);
+  const int64_t n = keys.num_rows;
+  const int grid = grid_for(t->device, p, std::max<int64_t>(n, 1), 256);
+  if (n > 0) {
+    if (keys.type == SJ_INT32) launch_stats<int32_t>(keys, grid, st, stream);
+    else launch_stats<int64_t>(keys, grid, st, stream);
+  }
+  BuildStats h{};
+  if (cudaMemcpyAsync(&h, st, sizeof(h), cudaMemcpyDeviceToHost, stream) != cudaSuccess ||
+      cudaStreamSynchronize(stream) != cudaSuccess)
+    return fail(set_error(SJ_ERR_DEVICE, std::string("build stats: ") + cudaGetErrorString(cudaGetLastError())));
+  t->valid_rows = (int64_t)h.n_valid;
+  t->null_rows = (int64_t)h.n_null;
+  if (t->valid_rows > 0) {
+    t->kmin = h.kmin;
+    t->kmax = h.kmax;
+  } else {
+    t->kmin = 0;
+    t->kmax = -1;
+  }
+
+  // Slot encoding: packed when (key - kmin) and the row id share 64 bits with the all-ones key
+  // field left unused, wide otherwise.
+  t->rid_bits = std::max(1, bit_width_u64((uint64_t)std::max<int64_t>(n - 1, 0)));
+  const uint64_t range = t->valid_rows > 0 ? (uint64_t)t->kmax - (uint64_t)t->kmin : 0;
+  const uint64_t key_field_max = (1ull << (64 - t->rid_bits)) - 1;  // all-ones = EMPTY marker
+  const bool packed_fits = range < key_field_max;
+  t->slot_kind = (packed_fits && !p.force_wide) ? SJ_SLOT_PACKED64 : SJ_SLOT_WIDE128;
+  const bool wide = t->slot_kind == SJ_SLOT_WIDE128;
+  const int spb = wide ? 2 : 4;
+
+  int log2_nb = log2_buckets_for(t->valid_rows, p.load_factor, spb);
+  log2_nb = std::max(log2_nb, std::min(t->pbits, 30));
+  if (log2_nb > 31) return fail(set_error(SJ_ERR_INVALID, "table too large"));
+  if (sj_status e = alloc_slots(t, log2_nb, stream)) return fail(e);
+
+  TableDev d = make_dev(t);
+  if (t->valid_rows > 0) {
+    if (keys.type == SJ_INT32) {
+      if (wide) launch_insert<int32_t, true>(d, keys, grid, st, stream);
+      else launch_insert<int32_t, false>(d, keys, grid, st, stream);
+    } else {
+      if (wide) launch_insert<int64_t, true>(d, keys, grid, st, stream);
+      else launch_insert<int64_t, false>(d, keys, grid, st, stream);
+    }
+  }
+  if (cudaMemcpyAsync(&h, st, sizeof(h), cudaMemcpyDeviceToHost, stream) != cudaSuccess ||
+      cudaStreamSynchronize(stream) != cudaSuccess)
+    return fail(set_error(SJ_ERR_DEVICE, std::string("build insert: ") + cudaGetErrorString(cudaGetLastError())));
+  if (h.full) return fail(set_error(SJ_ERR_TABLE_FULL, "a table segment ran out of slots"));
+  t->distinct = t->valid_rows - (int64_t)h.n_dup;
+
+  const bool null_group = t->null_eq == SJ_NULLS_EQUAL && t->null_rows > 0;
+  const bool grouped = p.layout == SJ_LAYOUT_GROUPED || h.n_dup > 0 || null_group;
+  if (p.layout == SJ_LAYOUT_DISTINCT && grouped)
+    return fail(set_error(SJ_ERR_INVALID, "layout DISTINCT requested but the build keys are not unique"));
+  t->layout = grouped ? SJ_LAYOUT_GROUPED : SJ_LAYOUT_DISTINCT;
+  t->max_group = 1;
+
+  if (grouped) {
+    // Shrink to the distinct keys when that saves at least 4x.
+    const int want = std::max(log2_buckets_for(t->distinct, p.load_factor, spb), std::min(t->pbits, 30));
+    if (want + 2 <= t->log2_nb) {
+      TableDev old = d;
+      void* old_slots = t->slots;
+      const size_t old_bytes = t->slots_bytes;
+      const uint64_t old_buckets = 1ull << t->log2_nb;
+      t->slots = nullptr;
+      if (sj_status e = alloc_slots(t, want, stream)) {
+        alloc.release(old_slots, old_bytes, stream);
+        return fail(e);
+      }
+      d = make_dev(t);
+      const int g2 = grid_for(t->device, p, (int64_t)old_buckets, 256);
+      if (wide) reinsert_kernel<true><<<g2, 256, 0, stream>>>(old, old_buckets, d, st);
+      else reinsert_kernel<false><<<g2, 256, 0, stream>>>(old, old_buckets, d, st);
+      alloc.release(old_slots, old_bytes, stream);
+    }
+    d = make_dev(t);  // now with null_group set for the grouped layout
+    const int64_t ns = t->num_slots();
+    const int64_t ngroups = ns + 1;  // + the NULL group
+    Scratch cnt_buf, tmp_buf;
+    if (sj_status e = cnt_buf.get(alloc, (size_t)ngroups * sizeof(int32_t), stream)) return fail(e);
+    if (sj_status e = tmp_buf.get(alloc, kScanBlocks * sizeof(int64_t), stream)) return fail(e);
+    int32_t* cnt = cnt_buf.as<int32_t>();
+    SJ_CUDA_TRY(cudaMemsetAsync(cnt, 0, (size_t)ngroups * sizeof(int32_t), stream));
+    t->grp_off_bytes = (size_t)(ngroups + 1) * sizeof(int32_t);
+    if (sj_status e = alloc.allocate((void**)&t->grp_off, t->grp_off_bytes, stream)) return fail(e);
+    const int64_t grouped_rows = t->valid_rows + (null_group ? t->null_rows : 0);
+    t->grp_rid_bytes = (size_t)std::max<int64_t>(grouped_rows, 1) * sizeof(int32_t);
+    if (sj_status e = alloc.allocate((void**)&t->grp_rid, t->grp_rid_bytes, stream)) return fail(e);
+    d = make_dev(t);
+    if (n > 0) {
+      if (keys.type == SJ_INT32) {
+        if (wide) launch_group<int32_t, true>(d, keys, grid, cnt, nullptr, nullptr, false, st, stream);
+        else launch_group<int32_t, false>(d, keys, grid, cnt, nullptr, nullptr, false, st, stream);
+      } else {
+        if (wide) launch_group<int64_t, true>(d, keys, grid, cnt, nullptr, nullptr, false, st, stream);
+        else launch_group<int64_t, false>(d, keys, grid, cnt, nullptr, nullptr, false, st, stream);
+      }
+    }
+    device_exclusive_scan<int32_t, int32_t>(cnt, t->grp_off, nullptr, ngroups, tmp_buf.as<int64_t>(), stream);
+    SJ_CUDA_TRY(cudaMemsetAsync(cnt, 0, (size_t)ngroups * sizeof(int32_t), stream));
+    if (n > 0) {
+      if (keys.type == SJ_INT32) {
+        if (wide) launch_group<int32_t, true>(d, keys, grid, cnt, t->grp_off, t->grp_rid, true, st, stream);
+        else launch_group<int32_t, false>(d, keys, grid, cnt, t->grp_off, t->grp_rid, true, st, stream);
+      } else {
+        if (wide) launch_group<int64_t, true>(d, keys, grid, cnt, t->grp_off, t->grp_rid, true, st, stream);
+        else launch_group<int64_t, false>(d, keys, grid, cnt, t->grp_off, t->grp_rid, true, st, stream);
+      }
+    }
+    if (cudaMemcpyAsync(&h, st, sizeof(h), cudaMemcpyDeviceToHost, stream) != cudaSuccess ||
+        cudaStreamSynchronize(stream) != cudaSuccess)
+      return fail(set_error(SJ_ERR_DEVICE, std::string("grouped build: ") + cudaGetErrorString(cudaGetLastError())));
+    if (h.full) return fail(set_error(SJ_ERR_TABLE_FULL, "a table segment ran out of slots"));
+    t->max_group = (int32_t)std::max<unsigned>(h.max_group, 1u);
+  }
+  SJ_CUDA_TRY(cudaGetLastError());
+  *out = t;
+  return SJ_OK;
+}
+
+sj_status destroy_table(sj_table* t, cudaStream_t stream) {
+  if (!t) return SJ_OK;
+  if (t->slots) t->alloc.release(t->slots, t->slots_bytes, stream);
+  if (t->grp_off) t->alloc.release(t->grp_off, t->grp_off_bytes, stream);
+  if (t->grp_rid) t->alloc.release(t->grp_rid, t->grp_rid_bytes, stream);
+  delete t;
+  return SJ_OK;
+}
+
+}  // namespace sj
+
+int64_t sj_table::num_slots() const {
+  return ((int64_t)1 << log2_nb) * (slot_kind == SJ_SLOT_WIDE128 ? 2 : 4);
+}

@@ -1,0 +1,125 @@
+// Host-side internals shared by the sj translation units (not part of the C ABI).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+#include <string>
+
+#include "sj/sj_join.h"
+
+namespace sj {
+
+// ---- errors --------------------------------------------------------------------------------
+// Every ABI entry point records a message for its thread before returning a failure status.
+sj_status set_error(sj_status st, const std::string& msg);
+void clear_error();
+
+#define SJ_CUDA_TRY(expr)                                                                     \
+  do {                                                                                        \
+    cudaError_t sj_e_ = (expr);                                                               \
+    if (sj_e_ != cudaSuccess) {                                                               \
+      return ::sj::set_error(SJ_ERR_DEVICE, std::string(#expr " failed: ") +                  \
+                                              cudaGetErrorString(sj_e_));                     \
+    }                                                                                         \
+  } while (0)
+
+#define SJ_TRY(expr)                  \
+  do {                                \
+    sj_status sj_s_ = (expr);         \
+    if (sj_s_ != SJ_OK) return sj_s_; \
+  } while (0)
+
+// ---- memory ----------------------------------------------------------------------------------
+// All device memory goes through the caller's sj_alloc (or cudaMallocAsync when it is NULL).
+struct Allocator {
+  sj_alloc a{};
+  bool use_default = true;
+  explicit Allocator(const sj_alloc* user = nullptr);
+  // Returns SJ_ERR_OOM (and records a message) when the allocation fails.
+  sj_status allocate(void** p, size_t bytes, cudaStream_t s) const;
+  void release(void* p, size_t bytes, cudaStream_t s) const;
+};
+
+// RAII scratch buffer released on scope exit (stream-ordered).
+struct Scratch {
+  const Allocator* alloc = nullptr;
+  cudaStream_t stream    = nullptr;
+  void* ptr              = nullptr;
+  size_t bytes           = 0;
+  Scratch() = default;
+  Scratch(const Scratch&) = delete;
+  Scratch& operator=(const Scratch&) = delete;
+  sj_status get(const Allocator& a, size_t n, cudaStream_t s) {
+    alloc = &a;
+    stream = s;
+    bytes = n < 16 ? 16 : n;
+    return a.allocate(&ptr, bytes, s);
+  }
+  ~Scratch() {
+    if (ptr) alloc->release(ptr, bytes, stream);
+  }
+  template <typename T>
+  T* as() const {
+    return static_cast<T*>(ptr);
+  }
+};
+
+int sm_count(int device);
+int type_width(int32_t t);  // bytes per element, 0 if invalid
+
+// ---- the table -------------------------------------------------------------------------------
+}  // namespace sj
+
+struct sj_table {
+  int device = 0;
+  sj::Allocator alloc;
+  int32_t key_type   = SJ_INT64;
+  int32_t layout     = SJ_LAYOUT_DISTINCT;
+  int32_t slot_kind  = SJ_SLOT_PACKED64;
+  int32_t null_eq    = SJ_NULLS_UNEQUAL;
+  int64_t build_rows = 0, valid_rows = 0, null_rows = 0, distinct = 0;
+  int64_t kmin = 0, kmax = -1;
+  int32_t rid_bits   = 1;
+  int32_t log2_nb    = 0;  // log2(#buckets)
+  int32_t seg_log2   = 0;  // log2(#buckets per probing segment); == log2_nb unless partitioned
+  int32_t pbits      = 0;  // radix bits of the partitioned variant
+  int32_t max_group  = 1;
+  void* slots        = nullptr;  // #buckets * 32 bytes
+  size_t slots_bytes = 0;
+  int32_t* grp_off   = nullptr;  // GROUPED: #slots + 2 offsets (group #slots = NULL keys)
+  size_t grp_off_bytes = 0;
+  int32_t* grp_rid   = nullptr;  // GROUPED: build row ids ordered by group
+  size_t grp_rid_bytes = 0;
+  sj_join_params params{};
+  int64_t num_slots() const;
+};
+
+namespace sj {
+
+// ---- kernel launchers (sj_build.cu / sj_probe.cu) ---------------------------------------------
+sj_status build_table(const sj_column& keys, const sj_join_params& p, const Allocator& alloc,
+                      cudaStream_t stream, sj_table** out);
+sj_status destroy_table(sj_table* t, cudaStream_t stream);
+
+struct GatherSpec {
+  const sj_column* probe_payload;
+  int32_t n_probe_payload;
+  const sj_column* build_payload;
+  int32_t n_build_payload;
+  int32_t* out_probe_rid;
+  int32_t* out_build_rid;
+  const sj_mut_column* out_probe_payload;
+  const sj_mut_column* out_build_payload;
+  int64_t capacity;
+};
+
+sj_status probe_count(const sj_table* t, const sj_column& probe, const Allocator& alloc,
+                      cudaStream_t stream, int64_t* d_count);
+sj_status probe_gather(const sj_table* t, const sj_column& probe, const GatherSpec& g,
+                       const Allocator& alloc, cudaStream_t stream, int64_t* d_count);
+
+sj_status validate_column(const sj_column* c, const char* what, bool key);
+
+}  // namespace sj

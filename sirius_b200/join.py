@@ -1,0 +1,227 @@
+"""Host-side API of the join over torch device tensors, calling the C ABI (``libsj.so``).
+
+``HashTable`` mirrors how Sirius's hash-join operator uses a built table
+(``src/op/sirius_physical_hash_join.cpp``): build once per partition (``:1593-1624``), then
+probe it many times, each probe followed by the payload gather (``gather_join_output``,
+``:1299-1359``). ``inner_join`` is the one-shot STANDARD-mode join (``cudf::inner_join`` at
+``:1872``). Output columns come in the operator's order: probe payloads, then build payloads.
+
+torch is used only for device memory and streams; every join step runs in ``libsj.so``.
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass, field
+from typing import Optional, Sequence
+
+import torch
+
+from . import _lib as L
+
+_TYPES = {
+    torch.int8: L.SJ_INT8, torch.int16: L.SJ_INT16, torch.int32: L.SJ_INT32, torch.int64: L.SJ_INT64,
+    torch.float32: L.SJ_FLOAT32, torch.float64: L.SJ_FLOAT64, torch.bool: L.SJ_BOOL8,
+    torch.uint32: L.SJ_UINT32, torch.uint64: L.SJ_UINT64,
+}
+
+
+def sj_type(dtype: torch.dtype) -> int:
+    try:
+        return _TYPES[dtype]
+    except KeyError:
+        raise TypeError(f"unsupported column dtype {dtype}") from None
+
+
+def _stream_handle(stream: Optional[torch.cuda.Stream]) -> int:
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return s.cuda_stream
+
+
+def _as_pair(c):
+    """A payload/key argument is a tensor or a (tensor, validity-words-or-None) pair."""
+    if isinstance(c, (tuple, list)):
+        return c[0], (c[1] if len(c) > 1 else None)
+    return c, None
+
+
+def make_column(data: torch.Tensor, validity: Optional[torch.Tensor] = None, validity_offset: int = 0) -> L.SjColumn:
+    if data.dim() != 1 or not data.is_contiguous():
+        raise ValueError("columns must be contiguous 1-D tensors")
+    if not data.is_cuda:
+        raise ValueError("columns must live on the GPU")
+    if validity is not None and (not validity.is_cuda or validity.dtype not in (torch.int32, torch.uint32)):
+        raise ValueError("validity must be a CUDA int32/uint32 tensor of bitmask words")
+    col = L.SjColumn()
+    col.data = data.data_ptr() if data.numel() else None
+    col.validity = validity.data_ptr() if validity is not None else None
+    col.validity_offset = validity_offset
+    col.num_rows = data.numel()
+    col.type = sj_type(data.dtype)
+    return col
+
+
+def _cols(cols: Sequence[L.SjColumn], cls=L.SjColumn):
+    arr = (cls * max(1, len(cols)))()
+    for i, c in enumerate(cols):
+        arr[i] = c
+    return arr
+
+
+@dataclass
+class JoinOutput:
+    """Result of an INNER probe + gather: ``count`` rows (the tensors may be longer)."""
+    count: int
+    probe_rid: Optional[torch.Tensor]
+    build_rid: Optional[torch.Tensor]
+    probe_payload: list = field(default_factory=list)
+    build_payload: list = field(default_factory=list)
+    probe_payload_validity: list = field(default_factory=list)
+    build_payload_validity: list = field(default_factory=list)
+
+    def trimmed(self) -> "JoinOutput":
+        n = self.count
+
+        def cut(t):
+            return None if t is None else t[:n]
+
+        def cutv(v):
+            return None if v is None else v[: (n + 31) // 32]
+        return JoinOutput(n, cut(self.probe_rid), cut(self.build_rid),
+                          [cut(t) for t in self.probe_payload], [cut(t) for t in self.build_payload],
+                          [cutv(v) for v in self.probe_payload_validity],
+                          [cutv(v) for v in self.build_payload_validity])
+
+
+def allocate_output(capacity: int, probe_payload=(), build_payload=(), device=None, rids=True) -> JoinOutput:
+    """Pre-allocate output buffers for ``capacity`` rows (payload dtypes/validity follow the inputs)."""
+    dev = device or torch.device("cuda")
+    words = (capacity + 31) // 32
+
+    def outs(cols):
+        data, val = [], []
+        for c in cols:
+            t, v = _as_pair(c)
+            data.append(torch.empty(capacity, dtype=t.dtype, device=dev))
+            val.append(torch.empty(words, dtype=torch.int32, device=dev) if v is not None else None)
+        return data, val
+    pd, pv = outs(probe_payload)
+    bd, bv = outs(build_payload)
+    prid = torch.empty(capacity, dtype=torch.int32, device=dev) if rids else None
+    brid = torch.empty(capacity, dtype=torch.int32, device=dev) if rids else None
+    return JoinOutput(0, prid, brid, pd, bd, pv, bv)
+
+
+def _mut(t: torch.Tensor, v: Optional[torch.Tensor]) -> L.SjMutColumn:
+    m = L.SjMutColumn()
+    m.data = t.data_ptr() if t.numel() else None
+    m.validity = v.data_ptr() if v is not None else None
+    m.type = sj_type(t.dtype)
+    return m
+
+
+class HashTable:
+    """A built table resident on the device (one partition slot of the BUILD_PROBE mode)."""
+
+    def __init__(self, keys: torch.Tensor, validity: Optional[torch.Tensor] = None, *,
+                 layout: int = L.SJ_LAYOUT_AUTO, null_equality: int = L.SJ_NULLS_UNEQUAL,
+                 load_factor: float = 0.5, partition_bits: int = 0, force_wide: bool = False,
+                 ctas_per_sm: int = 0, stream: Optional[torch.cuda.Stream] = None):
+        self._lib = L.load()
+        self._handle = ctypes.c_void_p()
+        self.keys = keys
+        self.params = L.default_params(layout=layout, null_equality=null_equality, load_factor=load_factor,
+                                       partition_bits=partition_bits, force_wide=int(force_wide))
+        if ctas_per_sm:
+            self.params.ctas_per_sm = ctas_per_sm
+        col = make_column(keys, validity)
+        st = self._lib.sj_build(ctypes.byref(col), 1, ctypes.byref(self.params), None,
+                                _stream_handle(stream), ctypes.byref(self._handle))
+        L.check(st, "sj_build")
+        self.build_rows = keys.numel()
+
+    @property
+    def handle(self):
+        if not self._handle:
+            raise RuntimeError("table is closed")
+        return self._handle
+
+    def info(self) -> L.SjTableInfo:
+        inf = L.SjTableInfo()
+        L.check(self._lib.sj_table_get_info(self.handle, ctypes.byref(inf)), "sj_table_get_info")
+        return inf
+
+    def count(self, probe_keys: torch.Tensor, probe_validity: Optional[torch.Tensor] = None,
+              stream: Optional[torch.cuda.Stream] = None, d_count: Optional[torch.Tensor] = None) -> torch.Tensor:
+        """Device int64[1] holding the number of INNER matches (stream-ordered)."""
+        col = make_column(probe_keys, probe_validity)
+        dc = d_count if d_count is not None else torch.empty(1, dtype=torch.int64, device=probe_keys.device)
+        L.check(self._lib.sj_probe_count(self.handle, ctypes.byref(col), 1, None, _stream_handle(stream),
+                                         dc.data_ptr()), "sj_probe_count")
+        return dc
+
+    def probe_gather(self, probe_keys: torch.Tensor, probe_validity: Optional[torch.Tensor] = None,
+                     probe_payload=(), build_payload=(), *, capacity: Optional[int] = None,
+                     out: Optional[JoinOutput] = None, d_count: Optional[torch.Tensor] = None,
+                     stream: Optional[torch.cuda.Stream] = None, sync: bool = True) -> JoinOutput:
+        """INNER probe fused with the payload gather.
+
+        ``capacity`` defaults to the exact count (one count pass + a sync) unless the table is
+        DISTINCT, where the probe row count is an upper bound. With ``sync=False`` the returned
+        ``count`` is -1 and the device count stays in ``d_count``.
+        """
+        dev = probe_keys.device
+        if capacity is None:
+            if out is not None:
+                capacity = out.probe_rid.numel() if out.probe_rid is not None else out.probe_payload[0].numel()
+            elif self.info().layout == L.SJ_LAYOUT_DISTINCT:
+                capacity = probe_keys.numel()
+            else:
+                capacity = int(self.count(probe_keys, probe_validity, stream).item())
+        if out is None:
+            out = allocate_output(capacity, probe_payload, build_payload, dev)
+        pin = [make_column(*_as_pair(c)) for c in probe_payload]
+        bin_ = [make_column(*_as_pair(c)) for c in build_payload]
+        pout = [_mut(t, v) for t, v in zip(out.probe_payload, out.probe_payload_validity)]
+        bout = [_mut(t, v) for t, v in zip(out.build_payload, out.build_payload_validity)]
+        dc = d_count if d_count is not None else torch.empty(1, dtype=torch.int64, device=dev)
+        key = make_column(probe_keys, probe_validity)
+        st = self._lib.sj_probe_gather(
+            self.handle, ctypes.byref(key), 1, _cols(pin), len(pin), _cols(bin_), len(bin_),
+            out.probe_rid.data_ptr() if out.probe_rid is not None else None,
+            out.build_rid.data_ptr() if out.build_rid is not None else None,
+            _cols(pout, L.SjMutColumn), _cols(bout, L.SjMutColumn), capacity, None, _stream_handle(stream),
+            dc.data_ptr())
+        L.check(st, "sj_probe_gather")
+        if not sync:
+            out.count = -1
+            return out
+        out.count = int(dc.item())
+        if out.count > capacity:
+            raise L.SjError(L.SJ_ERR_CAPACITY, "sj_probe_gather", f"{out.count} matches > capacity {capacity}")
+        return out
+
+    def close(self, stream: Optional[torch.cuda.Stream] = None):
+        if self._handle:
+            self._lib.sj_table_destroy(self._handle, _stream_handle(stream))
+            self._handle = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def inner_join(build_keys, probe_keys, build_validity=None, probe_validity=None, probe_payload=(),
+               build_payload=(), *, capacity: Optional[int] = None, **table_kwargs) -> JoinOutput:
+    """One-shot INNER join (build, probe, gather, free): STANDARD mode."""
+    stream = table_kwargs.pop("stream", None)
+    with HashTable(build_keys, build_validity, stream=stream, **table_kwargs) as t:
+        return t.probe_gather(probe_keys, probe_validity, probe_payload, build_payload, capacity=capacity,
+                              stream=stream).trimmed()

@@ -1,0 +1,103 @@
+"""The C ABI library loads on a CPU-only machine, exports every function the headers declare,
+and its struct layouts match both the C compiler's and the ctypes binding's. No GPU calls."""
+import ctypes
+import re
+import subprocess
+from pathlib import Path
+
+import pytest
+
+ROOT = Path(__file__).resolve().parent.parent
+HEADERS = sorted((ROOT / "include" / "sj").glob("*.h"))
+DECL = re.compile(r"SJ_EXPORT\s+[\w\s\*]+?\b(sj_\w+)\s*\(", re.S)
+
+
+def declared():
+    names = []
+    for h in HEADERS:
+        names += DECL.findall(h.read_text())
+    return sorted(set(names))
+
+
+def test_headers_declare_functions():
+    names = declared()
+    assert "sj_build" in names and "sj_probe_gather" in names
+    assert len(names) >= 10
+
+
+def test_every_declared_symbol_is_exported(built):
+    from sirius_b200 import _lib
+    lib = _lib.load()
+    missing = [n for n in declared() if not hasattr(lib, n)]
+    assert not missing, f"declared but not exported: {missing}"
+
+
+def test_binding_covers_every_declared_symbol(built):
+    from sirius_b200 import _lib
+    assert set(declared()) <= set(_lib.SIGNATURES) | set(getattr(_lib, "EXTRA_SIGNATURES", {}))
+
+
+def test_exports_are_only_the_abi(built):
+    out = subprocess.run(["nm", "-D", "--defined-only", str(ROOT / "sirius_b200" / "libsj.so")],
+                         capture_output=True, text=True, check=True).stdout
+    exported = sorted({l.split()[-1] for l in out.splitlines() if " T " in l})
+    assert all(s.startswith("sj_") for s in exported), exported
+
+
+def test_struct_layout_matches_c(built, tmp_path):
+    from sirius_b200 import _lib
+    src = tmp_path / "layout.c"
+    src.write_text(r'''
+#include <stdio.h>
+#include <stddef.h>
+#include "sj/sj_join.h"
+int main(void) {
+  printf("%zu %zu %zu %zu %zu\n", sizeof(sj_column), sizeof(sj_mut_column), sizeof(sj_alloc),
+         sizeof(sj_join_params), sizeof(sj_table_info));
+  printf("%zu %zu %zu\n", offsetof(sj_column, num_rows), offsetof(sj_join_params, ctas_per_sm),
+         offsetof(sj_table_info, max_group));
+  return 0;
+}
+''')
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-std=c11", f"-I{ROOT / 'include'}", str(src), "-o", str(exe)], check=True)
+    got = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()
+    exp = [ctypes.sizeof(_lib.SjColumn), ctypes.sizeof(_lib.SjMutColumn), ctypes.sizeof(_lib.SjAlloc),
+           ctypes.sizeof(_lib.SjJoinParams), ctypes.sizeof(_lib.SjTableInfo),
+           _lib.SjColumn.num_rows.offset, _lib.SjJoinParams.ctas_per_sm.offset, _lib.SjTableInfo.max_group.offset]
+    assert [int(x) for x in got] == exp
+
+
+def test_host_only_calls(built):
+    from sirius_b200 import _lib
+    lib = _lib.load()
+    p = _lib.default_params()
+    assert abs(p.load_factor - 0.5) < 1e-6 and p.layout == _lib.SJ_LAYOUT_AUTO
+    assert lib.sj_status_string(_lib.SJ_ERR_OOM) == b"SJ_ERR_OOM"
+    assert lib.sj_version() >= 100
+
+
+def test_argument_validation_needs_no_gpu(built):
+    """Bad arguments are rejected before any CUDA call."""
+    from sirius_b200 import _lib
+    lib = _lib.load()
+    col = _lib.SjColumn()
+    col.type = _lib.SJ_INT32
+    out = ctypes.c_void_p()
+    st = lib.sj_build(ctypes.byref(col), 2, None, None, None, ctypes.byref(out))
+    assert st == _lib.SJ_ERR_INVALID
+    assert b"one key column" in lib.sj_last_error()
+    col.type = _lib.SJ_FLOAT32
+    st = lib.sj_build(ctypes.byref(col), 1, None, None, None, ctypes.byref(out))
+    assert st == _lib.SJ_ERR_INVALID
+    assert b"INT32 or INT64" in lib.sj_last_error()
+    st = lib.sj_build(ctypes.byref(col), 1, None, None, None, None)
+    assert st == _lib.SJ_ERR_INVALID
+    with pytest.raises(_lib.SjError):
+        _lib.check(_lib.SJ_ERR_INVALID, "x")
+
+
+def test_library_missing_fails_loudly(tmp_path):
+    from sirius_b200 import _lib
+    with pytest.raises(FileNotFoundError):
+        _lib.load(tmp_path / "nope.so")

@@ -55,6 +55,7 @@ def parse():
     ap.add_argument("--cpu-steps", type=int, default=2)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--partition-bits", type=int, default=0)
+    ap.add_argument("--aggregation", type=int, default=0)
     return ap.parse_args()
 
 
@@ -83,60 +84,67 @@ def profile_traffic(kernel: str):
 
 
 class ClockSampler:
-    """nvidia-smi samples during the timed region."""
-    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    """SM clock and throttle reasons sampled through NVML every ~2 ms during the timed region
+    (nvidia-smi as a fallback). Reads only; changes no GPU setting."""
+    REASONS = {"hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20, "hw_thermal_slowdown": 0x40,
+               "sw_power_cap": 0x4}
 
     def __init__(self, index: int):
         self.index = index
-        self.proc = None
-        self.lines = []
-        self.t = None
+        self.samples = []
+        self.reasons = set()
+        self.max_mhz = None
+        self._stop = threading.Event()
+        self._t = None
+        self._nvml = None
 
     def __enter__(self):
         try:
-            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
-                                          "--format=csv,noheader,nounits", "-lms", "100"],
-                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.t = threading.Thread(target=self._read, daemon=True)
-            self.t.start()
+            import pynvml
+            pynvml.nvmlInit()
+            self._nvml = pynvml
+            self._h = pynvml.nvmlDeviceGetHandleByIndex(self.index)
+            self.max_mhz = float(pynvml.nvmlDeviceGetMaxClockInfo(self._h, pynvml.NVML_CLOCK_SM))
         except Exception:
-            self.proc = None
+            self._nvml = None
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
         return self
 
-    def _read(self):
-        for line in self.proc.stdout:
-            self.lines.append(line.strip())
+    def _run(self):
+        while not self._stop.is_set():
+            if self._nvml is not None:
+                try:
+                    self.samples.append(float(self._nvml.nvmlDeviceGetClockInfo(self._h, self._nvml.NVML_CLOCK_SM)))
+                    r = self._nvml.nvmlDeviceGetCurrentClocksEventReasons(self._h)
+                    for name, bit in self.REASONS.items():
+                        if r & bit:
+                            self.reasons.add(name)
+                except Exception:
+                    pass
+                time.sleep(0.002)
+            else:
+                try:
+                    out = subprocess.run(["nvidia-smi", f"--id={self.index}",
+                                          "--query-gpu=clocks.sm,clocks.max.sm", "--format=csv,noheader,nounits"],
+                                         capture_output=True, text=True, timeout=5).stdout.split(",")
+                    self.samples.append(float(out[0]))
+                    self.max_mhz = float(out[1])
+                except Exception:
+                    pass
+                time.sleep(0.05)
 
     def __exit__(self, *exc):
-        if self.proc:
-            self.proc.terminate()
-            try:
-                self.proc.wait(timeout=5)
-            except Exception:
-                self.proc.kill()
-            if self.t:
-                self.t.join(timeout=2)
+        self._stop.set()
+        if self._t:
+            self._t.join(timeout=2)
 
     def summary(self):
-        sm, mx, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for l in self.lines:
-            f = [x.strip() for x in l.split(",")]
-            if len(f) < 9:
-                continue
-            try:
-                sm.append(float(f[1]))
-                mx = float(f[2])
-            except ValueError:
-                continue
-            for n, v in zip(names, f[5:9]):
-                if v.lower().startswith("active"):
-                    reasons.add(n)
-        if not sm:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
-        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": self.max_mhz, "reasons": sorted(self.reasons), "samples": 0}
+        return {"sm_mhz": statistics.median(self.samples), "sm_max_mhz": self.max_mhz,
+                "reasons": sorted(self.reasons), "samples": len(self.samples),
+                "source": "nvml" if self._nvml is not None else "nvidia-smi"}
 
 
 def workload_desc(nb, np_):
@@ -240,7 +248,7 @@ def run_sj(args):
     for i in range(3):
         torch.cuda.synchronize()
         ev0.record()
-        tb = J.HashTable(bk, partition_bits=args.partition_bits)
+        tb = J.HashTable(bk, attach=bp, partition_bits=args.partition_bits, aggregation=args.aggregation)
         ev1.record()
         torch.cuda.synchronize()
         t_build.append(ev0.elapsed_time(ev1))
@@ -253,7 +261,7 @@ def run_sj(args):
     d_count = torch.zeros(1, dtype=torch.int64, device=dev)
 
     def step():
-        table.probe_gather(pk, None, pp, bp, capacity=args.n_probe, out=out, d_count=d_count, sync=False)
+        table.probe_gather(pk, None, pp, attached=True, capacity=args.n_probe, out=out, d_count=d_count, sync=False)
 
     for _ in range(max(3, args.warmup)):
         step()
@@ -271,6 +279,8 @@ def run_sj(args):
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
+    _lib.timing_collect()           # drop warm-up records
+    _lib.timing_enable(True)        # per-kernel CUDA events inside the library, on the launch stream
     starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
     ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
     with ClockSampler(dev.index) as clk:
@@ -283,6 +293,8 @@ def run_sj(args):
             ends[i].record()
         t_all1.record()
         torch.cuda.synchronize()
+    _lib.timing_enable(False)
+    kernel_times = _lib.timing_collect()
     if world > 1:
         dist.barrier()
     total_ms = t_all0.elapsed_time(t_all1)
@@ -315,8 +327,8 @@ def run_sj(args):
             d_pk.copy_(h_pk, non_blocking=True)
             for d, h in zip(d_bp + d_pp, h_bp + h_pp):
                 d.copy_(h, non_blocking=True)
-            with J.HashTable(d_bk) as tt:
-                tt.probe_gather(d_pk, None, d_pp, d_bp, capacity=args.n_probe, out=out, d_count=d_count,
+            with J.HashTable(d_bk, attach=d_bp, partition_bits=args.partition_bits) as tt:
+                tt.probe_gather(d_pk, None, d_pp, attached=True, capacity=args.n_probe, out=out, d_count=d_count,
                                 sync=False)
                 srcs = [out.probe_rid, out.build_rid] + out.probe_payload + out.build_payload
                 for h, s in zip(h_out, srcs):
@@ -344,15 +356,24 @@ def run_sj(args):
         e2e = {"value": round(args.n_probe * args.e2e_steps * world / (e_max / 1e3) / 1e6, 3),
                "unit": "Mtuples/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                "ms_per_step": round(e_max / args.e2e_steps, 3),
-               "what": "one-shot join from pinned host buffers: H2D of all inputs, sj_build, "
+               "what": "one-shot join from pinned host buffers: H2D of all inputs, sj_build_ex, "
                        "sj_probe_gather, D2H of the whole output"}
 
-    # ---- roofline of the probe kernel ----
+    # ---- roofline of the probe phase (the sj_probe_gather call) and its kernels ----
     alg = alg_bytes_probe_phase(inp)
     launch_ms = statistics.mean(per_launch)
     peak, peak_src = measured_peak()
     achieved = alg / (launch_ms / 1e3) / 1e9
-    traffic, traffic_src = profile_traffic("probe_distinct_kernel")
+    per_kernel = {}
+    for name, ms in kernel_times:
+        k = per_kernel.setdefault(name, [0, 0.0])
+        k[0] += 1
+        k[1] += ms
+    ktot = sum(v[1] for v in per_kernel.values()) or 1.0
+    kernels = {n: {"launches": c, "ms_per_launch": round(t / c, 4), "share": round(t / ktot, 4)}
+               for n, (c, t) in sorted(per_kernel.items(), key=lambda kv: -kv[1][1])}
+    dominant = next(iter(kernels), None)
+    traffic, traffic_src = profile_traffic("probe_phase")
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu and args.cpu_steps > 0:
@@ -382,13 +403,15 @@ def run_sj(args):
                        "t_build_ms": round(min(t_build), 3)},
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4), "traffic": traffic,
-                         "kernel": "probe_distinct_kernel", "alg_bytes_per_launch": int(alg),
-                         "launch_ms": round(launch_ms, 4), "peak_source": peak_src,
+                         "unit_of_work": "probe phase = one sj_probe_gather call over 64M probe rows "
+                                         "(partition + probe/gather kernels)",
+                         "alg_bytes_per_launch": int(alg), "launch_ms": round(launch_ms, 4),
+                         "dominant_kernel": dominant, "kernels": kernels, "peak_source": peak_src,
                          "frac_of_nominal_8TBs": round(achieved / NOMINAL_HBM_GBS, 4),
                          "traffic_source": traffic_src},
             "cpu_baseline": cpu,
             "e2e": e2e,
-            "gpu_launches": args.steps,
+            "gpu_launches": len(kernel_times),
             "clocks": clocks,
         }
         print(json.dumps(line), flush=True)

@@ -125,6 +125,11 @@ typedef enum sj_slot_kind {
   SJ_SLOT_WIDE128  = 1  /* {int64 key, row id} pair, inserted by 128-bit atomicCAS */
 } sj_slot_kind;
 
+/* Output reservation of the single-pass probe: matches are always compacted warp-aggregated
+ * (prefix over the lanes' hit counts); the range is then reserved with one atomicAdd per warp or
+ * one per CTA tile. AUTO picks per-CTA for probes of 2^20 rows or more. */
+typedef enum sj_aggregation { SJ_AGG_AUTO = 0, SJ_AGG_WARP = 1, SJ_AGG_CTA = 2 } sj_aggregation;
+
 /* Tunables. Zero-initialised fields take defaults (sj_default_params fills them in). */
 typedef struct sj_join_params {
   int32_t layout;           /* sj_layout */
@@ -132,10 +137,13 @@ typedef struct sj_join_params {
   float load_factor;        /* slots in use / slots; default 0.5 (the distinct_hash_join value) */
   int32_t block_size;       /* threads per CTA for probe kernels; default 256 */
   int32_t group_width;      /* probe group width 1,2,4,8,16,32 lanes per key; default 1 */
-  int32_t partition_bits;   /* radix bits of the partitioned variant; 0 = not partitioned */
+  int32_t partition_bits;   /* radix bits of the partitioned variant: 0 = automatic (partition
+                               when the table and its attached payloads outgrow L2), -1 = never,
+                               1..10 = that many bits (2^bits partitions) */
   int32_t force_wide;       /* 1 = use SJ_SLOT_WIDE128 even when the packed encoding fits */
   int32_t ctas_per_sm;      /* grid = ctas_per_sm * SM count for grid-stride kernels; default 4 */
-  int32_t reserved[8];
+  int32_t aggregation;      /* sj_aggregation: how probe matches reserve output positions */
+  int32_t reserved[7];
 } sj_join_params;
 
 typedef struct sj_table sj_table;
@@ -153,7 +161,7 @@ typedef struct sj_table_info {
   int32_t slot_kind;       /* sj_slot_kind */
   int32_t rid_bits;        /* row-id bits of a packed slot */
   int32_t key_type;        /* sj_type of the key */
-  int32_t partition_bits;  /* radix bits (0 = not partitioned) */
+  int32_t partition_bits;  /* radix bits used (0 = not partitioned) */
   int32_t max_group;       /* largest number of build rows sharing one key */
 } sj_table_info;
 
@@ -174,6 +182,17 @@ SJ_EXPORT void sj_default_params(sj_join_params* params);
 SJ_EXPORT sj_status sj_build(const sj_column* keys, int32_t num_keys, const sj_join_params* params,
                              const sj_alloc* alloc, sj_stream_t stream, sj_table** out);
 
+/* sj_build plus attached build payload columns (the build-side columns the operator projects,
+ * rhs_output_columns, src/op/sirius_physical_hash_join.cpp:1339-1353). The table keeps its own
+ * copy of them in table-position order, so a probe's payload gather reads the rows stored next to
+ * the matched slot's partition instead of the build batch at random; pass build_payload = NULL to
+ * sj_probe_gather to gather them. With radix partitioning (large tables) positions follow
+ * partition order and every partition's slots and payload rows stay L2-resident while its probes
+ * run. Costs one copy of the attached columns in device memory. */
+SJ_EXPORT sj_status sj_build_ex(const sj_column* keys, int32_t num_keys, const sj_column* payload,
+                                int32_t num_payload, const sj_join_params* params, const sj_alloc* alloc,
+                                sj_stream_t stream, sj_table** out);
+
 /* Free the table's device memory, stream-ordered on `stream` (on_finalize_operator frees each
  * slot's table on its device, src/op/sirius_physical_hash_join.cpp:2084-2097). */
 SJ_EXPORT sj_status sj_table_destroy(sj_table* table, sj_stream_t stream);
@@ -193,6 +212,8 @@ SJ_EXPORT sj_status sj_probe_count(const sj_table* table, const sj_column* probe
  *   out_probe_payload[c][p] = probe_payload[c][i]
  *   out_build_payload[c][p] = build_payload[c][j]
  * and validity bits copied from the payload columns (NULLIFY is not needed for INNER).
+ * build_payload == NULL with num_build_payload == the number of columns attached by sj_build_ex
+ * gathers the attached columns (in attach order) instead of caller columns.
  * *d_count (device int64) receives the total number of matches M; only positions p < capacity
  * are written, so the call succeeded iff M <= capacity (read *d_count after the stream).
  * A DISTINCT table never has M > probe rows. Output order is unspecified, as cuDF's is.
@@ -226,6 +247,19 @@ SJ_EXPORT const char* sj_status_string(sj_status status);
 
 /* Message of the last failing call on this thread ("" if none). */
 SJ_EXPORT const char* sj_last_error(void);
+
+/* Opt-in per-kernel timing. While enabled (process-wide), every kernel the library launches from
+ * the calling thread is bracketed by a CUDA event pair on its stream; sj_timing_collect waits for
+ * those events, writes up to `capacity` (name, milliseconds) records in launch order, clears the
+ * log and returns the number of records. Names are static strings. Off by default. */
+typedef struct sj_kernel_time {
+  const char* name;
+  float ms;
+  int32_t reserved;
+} sj_kernel_time;
+
+SJ_EXPORT void sj_timing_enable(int32_t on);
+SJ_EXPORT int32_t sj_timing_collect(sj_kernel_time* out, int32_t capacity);
 
 /* ABI version: major * 10000 + minor * 100 + patch. */
 SJ_EXPORT int32_t sj_version(void);

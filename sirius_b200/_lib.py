@@ -21,6 +21,7 @@ SJ_INT8, SJ_INT16, SJ_INT32, SJ_INT64, SJ_FLOAT32, SJ_FLOAT64, SJ_BOOL8, SJ_UINT
 SJ_LAYOUT_AUTO, SJ_LAYOUT_DISTINCT, SJ_LAYOUT_GROUPED = 0, 1, 2
 SJ_NULLS_UNEQUAL, SJ_NULLS_EQUAL = 0, 1
 SJ_SLOT_PACKED64, SJ_SLOT_WIDE128 = 0, 1
+SJ_AGG_AUTO, SJ_AGG_WARP, SJ_AGG_CTA = 0, 1, 2
 
 
 class SjColumn(Structure):
@@ -43,7 +44,8 @@ class SjAlloc(Structure):
 class SjJoinParams(Structure):
     _fields_ = [("layout", c_int32), ("null_equality", c_int32), ("load_factor", c_float),
                 ("block_size", c_int32), ("group_width", c_int32), ("partition_bits", c_int32),
-                ("force_wide", c_int32), ("ctas_per_sm", c_int32), ("reserved", c_int32 * 8)]
+                ("force_wide", c_int32), ("ctas_per_sm", c_int32), ("aggregation", c_int32),
+                ("reserved", c_int32 * 7)]
 
 
 class SjTableInfo(Structure):
@@ -54,11 +56,17 @@ class SjTableInfo(Structure):
                 ("max_group", c_int32)]
 
 
+class SjKernelTime(Structure):
+    _fields_ = [("name", c_char_p), ("ms", c_float), ("reserved", c_int32)]
+
+
 # (name, restype, argtypes) of every function the header declares.
 _P = POINTER
 SIGNATURES = {
     "sj_default_params": (None, [_P(SjJoinParams)]),
     "sj_build": (c_int32, [_P(SjColumn), c_int32, _P(SjJoinParams), _P(SjAlloc), c_void_p, _P(c_void_p)]),
+    "sj_build_ex": (c_int32, [_P(SjColumn), c_int32, _P(SjColumn), c_int32, _P(SjJoinParams), _P(SjAlloc), c_void_p,
+                              _P(c_void_p)]),
     "sj_table_destroy": (c_int32, [c_void_p, c_void_p]),
     "sj_table_get_info": (c_int32, [c_void_p, _P(SjTableInfo)]),
     "sj_probe_count": (c_int32, [c_void_p, _P(SjColumn), c_int32, _P(SjAlloc), c_void_p, c_void_p]),
@@ -71,6 +79,8 @@ SIGNATURES = {
     "sj_status_string": (c_char_p, [c_int32]),
     "sj_last_error": (c_char_p, []),
     "sj_version": (c_int32, []),
+    "sj_timing_enable": (None, [c_int32]),
+    "sj_timing_collect": (c_int32, [_P(SjKernelTime), c_int32]),
 }
 
 _lib = None
@@ -119,3 +129,14 @@ def default_params(**overrides) -> SjJoinParams:
     for k, v in overrides.items():
         setattr(p, k, v)
     return p
+
+
+def timing_enable(on: bool = True):
+    load().sj_timing_enable(int(on))
+
+
+def timing_collect(capacity: int = 4096):
+    """[(kernel name, ms)] recorded on this thread since the last collect (waits for the events)."""
+    buf = (SjKernelTime * capacity)()
+    n = load().sj_timing_collect(buf, capacity)
+    return [(buf[i].name.decode(), float(buf[i].ms)) for i in range(min(n, capacity))]

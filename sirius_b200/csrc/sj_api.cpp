@@ -2,6 +2,8 @@
 // arguments, converts C++ failures into sj_status + a per-thread message, and never throws.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+#include <atomic>
 #include <cstring>
 #include <mutex>
 #include <new>
@@ -27,10 +29,30 @@ Allocator::Allocator(const sj_alloc* user) {
   }
 }
 
+// The default allocator keeps freed blocks in the device's default memory pool (release threshold
+// = unlimited) so per-call scratch is recycled instead of returned to the driver at every sync.
+static void keep_default_pool(cudaStream_t s) {
+  static std::mutex mu;
+  static std::vector<char> done;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return;
+  std::lock_guard<std::mutex> lk(mu);
+  if ((int)done.size() <= dev) done.resize(dev + 1, 0);
+  if (done[dev]) return;
+  done[dev] = 1;
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+    uint64_t thr = ~0ull;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+  }
+  (void)s;
+}
+
 sj_status Allocator::allocate(void** p, size_t bytes, cudaStream_t s) const {
   *p = nullptr;
   if (bytes == 0) bytes = 16;
   if (use_default) {
+    keep_default_pool(s);
     cudaError_t e = cudaMallocAsync(p, bytes, s);
     if (e != cudaSuccess || *p == nullptr) {
       cudaGetLastError();  // clear the non-sticky allocation error
@@ -49,6 +71,41 @@ void Allocator::release(void* p, size_t bytes, cudaStream_t s) const {
   if (bytes == 0) bytes = 16;
   if (use_default) cudaFreeAsync(p, s);
   else a.free(a.ctx, p, bytes, reinterpret_cast<sj_stream_t>(s));
+}
+
+// ---- per-kernel timing --------------------------------------------------------------------
+static std::atomic<bool> g_timing{false};
+struct TimingRecord {
+  const char* name;
+  cudaEvent_t a, b;
+};
+static thread_local std::vector<TimingRecord> t_records;
+static thread_local std::vector<cudaEvent_t> t_event_pool;
+
+static cudaEvent_t pooled_event() {
+  if (!t_event_pool.empty()) {
+    cudaEvent_t e = t_event_pool.back();
+    t_event_pool.pop_back();
+    return e;
+  }
+  cudaEvent_t e = nullptr;
+  if (cudaEventCreate(&e) != cudaSuccess) return nullptr;
+  return e;
+}
+
+bool timing_enabled() { return g_timing.load(std::memory_order_relaxed); }
+
+KernelTimer::KernelTimer(const char* name, cudaStream_t s) : stream(s) {
+  if (!timing_enabled()) return;
+  cudaEvent_t a = pooled_event(), b = pooled_event();
+  if (!a || !b) return;
+  cudaEventRecord(a, s);
+  t_records.push_back(TimingRecord{name, a, b});
+  idx = (int)t_records.size() - 1;
+}
+
+KernelTimer::~KernelTimer() {
+  if (idx >= 0 && idx < (int)t_records.size()) cudaEventRecord(t_records[idx].b, stream);
 }
 
 int sm_count(int device) {
@@ -110,6 +167,7 @@ static sj_join_params resolve(const sj_join_params* p) {
   r.partition_bits = p->partition_bits;
   r.force_wide = p->force_wide;
   if (p->ctas_per_sm > 0) r.ctas_per_sm = p->ctas_per_sm;
+  r.aggregation = p->aggregation;
   return r;
 }
 
@@ -141,7 +199,26 @@ SJ_EXPORT sj_status sj_build(const sj_column* keys, int32_t num_keys, const sj_j
   if (!keys) return set_error(SJ_ERR_INVALID, "keys is NULL");
   try {
     const sj_join_params p = resolve(params);
-    return build_table(keys[0], p, Allocator(alloc), reinterpret_cast<cudaStream_t>(stream), out);
+    return build_table(keys[0], nullptr, 0, p, Allocator(alloc), reinterpret_cast<cudaStream_t>(stream), out);
+  } catch (const std::bad_alloc&) {
+    return set_error(SJ_ERR_OOM, "host allocation failed");
+  } catch (const std::exception& e) {
+    return set_error(SJ_ERR_DEVICE, e.what());
+  }
+}
+
+SJ_EXPORT sj_status sj_build_ex(const sj_column* keys, int32_t num_keys, const sj_column* payload,
+                                int32_t num_payload, const sj_join_params* params, const sj_alloc* alloc,
+                                sj_stream_t stream, sj_table** out) {
+  clear_error();
+  if (!out) return set_error(SJ_ERR_INVALID, "out is NULL");
+  *out = nullptr;
+  if (num_keys != 1) return set_error(SJ_ERR_INVALID, "exactly one key column is supported");
+  if (!keys) return set_error(SJ_ERR_INVALID, "keys is NULL");
+  try {
+    const sj_join_params p = resolve(params);
+    return build_table(keys[0], payload, num_payload, p, Allocator(alloc), reinterpret_cast<cudaStream_t>(stream),
+                       out);
   } catch (const std::bad_alloc&) {
     return set_error(SJ_ERR_OOM, "host allocation failed");
   } catch (const std::exception& e) {
@@ -163,7 +240,10 @@ SJ_EXPORT sj_status sj_table_get_info(const sj_table* t, sj_table_info* info) {
   info->null_rows = t->null_rows;
   info->distinct_keys = t->distinct;
   info->num_slots = t->num_slots();
-  info->device_bytes = (int64_t)(t->slots_bytes + t->grp_off_bytes + t->grp_rid_bytes);
+  size_t bytes = t->slots_bytes + t->grp_off_bytes + t->grp_rid_bytes + t->arow_bytes;
+  if (t->apay_owned)
+    for (int c = 0; c < t->n_attached; ++c) bytes += t->apay_bytes[c] + t->apay_valid_bytes[c];
+  info->device_bytes = (int64_t)bytes;
   info->key_min = t->valid_rows ? t->kmin : 0;
   info->key_max = t->valid_rows ? t->kmax : -1;
   info->layout = t->layout;
@@ -240,6 +320,25 @@ SJ_EXPORT const char* sj_status_string(sj_status s) {
 }
 
 SJ_EXPORT const char* sj_last_error(void) { return g_last_error.c_str(); }
+
+SJ_EXPORT void sj_timing_enable(int32_t on) { g_timing.store(on != 0); }
+
+SJ_EXPORT int32_t sj_timing_collect(sj_kernel_time* out, int32_t capacity) {
+  const int32_t n = (int32_t)t_records.size();
+  for (int32_t i = 0; i < n; ++i) {
+    TimingRecord& r = t_records[i];
+    float ms = -1.0f;
+    if (cudaEventSynchronize(r.b) == cudaSuccess) cudaEventElapsedTime(&ms, r.a, r.b);
+    if (out && i < capacity) {
+      out[i].name = r.name;
+      out[i].ms = ms;
+    }
+    t_event_pool.push_back(r.a);
+    t_event_pool.push_back(r.b);
+  }
+  t_records.clear();
+  return n;
+}
 
 SJ_EXPORT int32_t sj_version(void) { return 100; }
 

@@ -18,8 +18,12 @@
 #include <climits>
 #include <cstring>
 
+#include <cmath>
+#include <type_traits>
+
 #include "sj_device.cuh"
 #include "sj_internal.h"
+#include "sj_partition.cuh"
 #include "sj_scan.cuh"
 
 namespace sj {
@@ -334,8 +338,35 @@ static int log2_buckets_for(int64_t keys, double lf, int slots_per_bucket) {
   return l;
 }
 
-sj_status build_table(const sj_column& keys, const sj_join_params& p, const Allocator& alloc,
-                      cudaStream_t stream, sj_table** out) {
+// Radix bits chosen from the bytes a probe touches at random (table slots + position map +
+// attached payloads): none while that fits comfortably in L2, else enough partitions that one
+// partition's share is ~16 MB, so the partitions the GPU works on at any moment stay L2-resident.
+int auto_partition_bits(size_t random_bytes) {
+  const size_t kFitsL2 = 40ull << 20, kPerPartition = 16ull << 20;
+  if (random_bytes <= kFitsL2) return 0;
+  int b = 0;
+  while (((size_t)1 << b) * kPerPartition < random_bytes && b < kMaxPartitionBits) ++b;
+  return b;
+}
+
+__global__ void bits_to_bytes_kernel(const uint32_t* bits, int64_t off, int64_t n, uint8_t* out) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    out[i] = bit_valid(bits, off, i) ? 1 : 0;
+}
+
+template <typename Fn>
+static void by_type(int32_t key_type, bool wide, Fn&& fn) {
+  if (key_type == SJ_INT32) {
+    if (wide) fn(int32_t{}, std::true_type{});
+    else fn(int32_t{}, std::false_type{});
+  } else {
+    if (wide) fn(int64_t{}, std::true_type{});
+    else fn(int64_t{}, std::false_type{});
+  }
+}
+
+sj_status build_table(const sj_column& keys, const sj_column* payload, int32_t n_payload, const sj_join_params& p,
+                      const Allocator& alloc, cudaStream_t stream, sj_table** out) {
   SJ_TRY(validate_column(&keys, "build key", true));
   if (keys.num_rows > INT32_MAX)
     return set_error(SJ_ERR_INVALID, "build side exceeds the int32 row-id range");
@@ -343,8 +374,15 @@ sj_status build_table(const sj_column& keys, const sj_join_params& p, const Allo
     return set_error(SJ_ERR_INVALID, "load_factor must be in (0, 1)");
   if (p.layout < SJ_LAYOUT_AUTO || p.layout > SJ_LAYOUT_GROUPED)
     return set_error(SJ_ERR_INVALID, "unknown layout");
-  if (p.partition_bits < 0 || p.partition_bits > 16)
-    return set_error(SJ_ERR_INVALID, "partition_bits must be in [0, 16]");
+  if (p.partition_bits < -1 || p.partition_bits > kMaxPartitionBits)
+    return set_error(SJ_ERR_INVALID, "partition_bits must be 0 (automatic), -1 (never) or in [1, 10]");
+  if (n_payload < 0 || n_payload > kMaxPayload || (n_payload > 0 && payload == nullptr))
+    return set_error(SJ_ERR_INVALID, "at most 8 attached payload columns");
+  for (int c = 0; c < n_payload; ++c) {
+    SJ_TRY(validate_column(&payload[c], "attached build payload", false));
+    if (payload[c].num_rows != keys.num_rows)
+      return set_error(SJ_ERR_INVALID, "attached build payload row count differs from the key column");
+  }
 
   sj_table* t = new sj_table();
   t->alloc = alloc;
@@ -352,7 +390,6 @@ sj_status build_table(const sj_column& keys, const sj_join_params& p, const Allo
   t->key_type = keys.type;
   t->null_eq = p.null_equality;
   t->params = p;
-  t->pbits = p.partition_bits;
   t->build_rows = keys.num_rows;
   auto fail = [&](sj_status st) {
     destroy_table(t, stream);
@@ -383,8 +420,8 @@ sj_status build_table(const sj_column& keys, const sj_join_params& p, const Allo
     t->kmax = -1;
   }
 
-  // Slot encoding: packed when (key - kmin) and the row id share 64 bits with the all-ones key
-  // field left unused, wide otherwise.
+  // Slot encoding: packed when (key - kmin) and the row position share 64 bits with the all-ones
+  // key field left unused, wide otherwise.
   t->rid_bits = std::max(1, bit_width_u64((uint64_t)std::max<int64_t>(n - 1, 0)));
   const uint64_t range = t->valid_rows > 0 ? (uint64_t)t->kmax - (uint64_t)t->kmin : 0;
   const uint64_t key_field_max = (1ull << (64 - t->rid_bits)) - 1;  // all-ones = EMPTY marker
@@ -392,21 +429,109 @@ sj_status build_table(const sj_column& keys, const sj_join_params& p, const Allo
   t->slot_kind = (packed_fits && !p.force_wide) ? SJ_SLOT_PACKED64 : SJ_SLOT_WIDE128;
   const bool wide = t->slot_kind == SJ_SLOT_WIDE128;
   const int spb = wide ? 2 : 4;
-
   int log2_nb = log2_buckets_for(t->valid_rows, p.load_factor, spb);
-  log2_nb = std::max(log2_nb, std::min(t->pbits, 30));
   if (log2_nb > 31) return fail(set_error(SJ_ERR_INVALID, "table too large"));
+
+  // Partitioning (radix bits) and positions.
+  const bool null_group = t->null_eq == SJ_NULLS_EQUAL && t->null_rows > 0;
+  size_t pay_row_bytes = 0;
+  for (int c = 0; c < n_payload; ++c) pay_row_bytes += (size_t)type_width(payload[c].type);
+  // bytes a probe touches at random: slots + one row-store record per valid row (row id,
+  // validity bytes, payload fields, rounded up to a power of two)
+  size_t rec_bytes = 4 + pay_row_bytes + (size_t)n_payload;
+  size_t rec = 4;
+  while (rec < rec_bytes) rec <<= 1;
+  const size_t random_bytes = ((size_t)1 << log2_nb) * kBucketBytes + (size_t)t->valid_rows * rec;
+  int pbits = p.partition_bits == 0 ? auto_partition_bits(random_bytes) : std::max(0, p.partition_bits);
+  if (null_group) pbits = 0;  // NULL-key rows stay addressable by row id for the NULL group
+  pbits = std::min(pbits, log2_nb);
+  t->pbits = pbits;
+  t->params.partition_bits = pbits;
+  const bool use_pos = !null_group && t->valid_rows > 0 && (pbits > 0 || n_payload > 0);
   if (sj_status e = alloc_slots(t, log2_nb, stream)) return fail(e);
+
+  t->n_attached = n_payload;
+  for (int c = 0; c < n_payload; ++c) t->apay_type[c] = payload[c].type;
+  const int kw = keys.type == SJ_INT32 ? 4 : 8;
+  // key source of the insert / grouped passes: the caller's column, or its partitioned copy
+  sj_column src = keys;
+  Scratch part_keys, part_scratch;
+  if (use_pos) {
+    const int64_t nv = t->valid_rows;
+    if (sj_status e = part_keys.get(alloc, (size_t)nv * kw, stream)) return fail(e);
+    if (sj_status e = part_scratch.get(alloc, partition_scratch_bytes(pbits, t->device), stream)) return fail(e);
+    // row-store record layout
+    int off = 4;  // build row id
+    int voff[kMaxPayload], poff[kMaxPayload];
+    for (int c = 0; c < n_payload; ++c) voff[c] = payload[c].validity ? off++ : -1;
+    for (int c = 0; c < n_payload; ++c) {
+      const int w = type_width(payload[c].type);
+      off = (off + w - 1) / w * w;
+      poff[c] = off;
+      off += w;
+    }
+    int rec = 4;
+    while (rec < off && rec < 64) rec <<= 1;
+    if (rec < off) rec = (off + 15) / 16 * 16;
+    t->arow_stride = rec;
+    t->arow_bytes = (size_t)nv * rec;
+    if (sj_status e = alloc.allocate(&t->arow, t->arow_bytes, stream)) return fail(e);
+    char* arow = static_cast<char*>(t->arow);
+    t->pos_rid = reinterpret_cast<int32_t*>(arow);
+    t->pos_stride = rec;
+    PartSrc ps{};
+    PartDst pd{};
+    ps.keys = keys.data;
+    ps.kvalid = keys.validity;
+    ps.kvoff = keys.validity_offset;
+    ps.n = n;
+    ps.n_pay = n_payload;
+    pd.keys = part_keys.ptr;
+    pd.rid = t->pos_rid;
+    pd.stride = rec;
+    for (int c = 0; c < n_payload; ++c) {
+      const int w = type_width(payload[c].type);
+      ps.pay[c] = column_payload(payload[c].data, payload[c].validity, payload[c].validity_offset, w);
+      t->apay[c] = arow + poff[c];
+      t->apay_stride[c] = rec;
+      t->apay_valid[c] = voff[c] >= 0 ? reinterpret_cast<uint8_t*>(arow + voff[c]) : nullptr;
+      t->apay_vstride[c] = rec;
+      pd.pay[c] = t->apay[c];
+      pd.valid8[c] = t->apay_valid[c];
+    }
+    const int64_t *d_total, *d_offs;
+    int G;
+    if (sj_status e = radix_partition(ps, keys.type, pbits, pd, part_scratch.ptr, t->device, stream, &d_total,
+                                      &d_offs, &G))
+      return fail(e);
+    src = sj_column{part_keys.ptr, nullptr, 0, nv, keys.type, 0};
+  } else if (n_payload > 0) {
+    // positions are row ids: attach owned row-ordered column copies
+    t->apay_owned = true;
+    for (int c = 0; c < n_payload; ++c) {
+      const int w = type_width(payload[c].type);
+      t->apay_bytes[c] = (size_t)std::max<int64_t>(n, 1) * w;
+      t->apay_stride[c] = w;
+      t->apay_vstride[c] = 1;
+      if (sj_status e = alloc.allocate(&t->apay[c], t->apay_bytes[c], stream)) return fail(e);
+      if (n > 0) SJ_CUDA_TRY(cudaMemcpyAsync(t->apay[c], payload[c].data, (size_t)n * w, cudaMemcpyDeviceToDevice, stream));
+      if (payload[c].validity) {
+        t->apay_valid_bytes[c] = (size_t)std::max<int64_t>(n, 1);
+        if (sj_status e = alloc.allocate((void**)&t->apay_valid[c], t->apay_valid_bytes[c], stream)) return fail(e);
+        if (n > 0)
+          bits_to_bytes_kernel<<<grid, 256, 0, stream>>>(payload[c].validity, payload[c].validity_offset, n,
+                                                         t->apay_valid[c]);
+      }
+    }
+  }
+  const int64_t sn = src.num_rows;
+  const int sgrid = grid_for(t->device, p, std::max<int64_t>(sn, 1), 256);
 
   TableDev d = make_dev(t);
   if (t->valid_rows > 0) {
-    if (keys.type == SJ_INT32) {
-      if (wide) launch_insert<int32_t, true>(d, keys, grid, st, stream);
-      else launch_insert<int32_t, false>(d, keys, grid, st, stream);
-    } else {
-      if (wide) launch_insert<int64_t, true>(d, keys, grid, st, stream);
-      else launch_insert<int64_t, false>(d, keys, grid, st, stream);
-    }
+    by_type(keys.type, wide, [&](auto k, auto w) {
+      launch_insert<decltype(k), decltype(w)::value>(d, src, sgrid, st, stream);
+    });
   }
   if (cudaMemcpyAsync(&h, st, sizeof(h), cudaMemcpyDeviceToHost, stream) != cudaSuccess ||
       cudaStreamSynchronize(stream) != cudaSuccess)
@@ -414,7 +539,6 @@ sj_status build_table(const sj_column& keys, const sj_join_params& p, const Allo
   if (h.full) return fail(set_error(SJ_ERR_TABLE_FULL, "a table segment ran out of slots"));
   t->distinct = t->valid_rows - (int64_t)h.n_dup;
 
-  const bool null_group = t->null_eq == SJ_NULLS_EQUAL && t->null_rows > 0;
   const bool grouped = p.layout == SJ_LAYOUT_GROUPED || h.n_dup > 0 || null_group;
   if (p.layout == SJ_LAYOUT_DISTINCT && grouped)
     return fail(set_error(SJ_ERR_INVALID, "layout DISTINCT requested but the build keys are not unique"));
@@ -422,8 +546,8 @@ sj_status build_table(const sj_column& keys, const sj_join_params& p, const Allo
   t->max_group = 1;
 
   if (grouped) {
-    // Shrink to the distinct keys when that saves at least 4x.
-    const int want = std::max(log2_buckets_for(t->distinct, p.load_factor, spb), std::min(t->pbits, 30));
+    // Shrink to the distinct keys when that saves at least 4x (keeping the partition bits).
+    const int want = std::max(log2_buckets_for(t->distinct, p.load_factor, spb), t->pbits);
     if (want + 2 <= t->log2_nb) {
       TableDev old = d;
       void* old_slots = t->slots;
@@ -440,7 +564,6 @@ sj_status build_table(const sj_column& keys, const sj_join_params& p, const Allo
       else reinsert_kernel<false><<<g2, 256, 0, stream>>>(old, old_buckets, d, st);
       alloc.release(old_slots, old_bytes, stream);
     }
-    d = make_dev(t);  // now with null_group set for the grouped layout
     const int64_t ns = t->num_slots();
     const int64_t ngroups = ns + 1;  // + the NULL group
     Scratch cnt_buf, tmp_buf;
@@ -454,26 +577,16 @@ sj_status build_table(const sj_column& keys, const sj_join_params& p, const Allo
     t->grp_rid_bytes = (size_t)std::max<int64_t>(grouped_rows, 1) * sizeof(int32_t);
     if (sj_status e = alloc.allocate((void**)&t->grp_rid, t->grp_rid_bytes, stream)) return fail(e);
     d = make_dev(t);
-    if (n > 0) {
-      if (keys.type == SJ_INT32) {
-        if (wide) launch_group<int32_t, true>(d, keys, grid, cnt, nullptr, nullptr, false, st, stream);
-        else launch_group<int32_t, false>(d, keys, grid, cnt, nullptr, nullptr, false, st, stream);
-      } else {
-        if (wide) launch_group<int64_t, true>(d, keys, grid, cnt, nullptr, nullptr, false, st, stream);
-        else launch_group<int64_t, false>(d, keys, grid, cnt, nullptr, nullptr, false, st, stream);
-      }
-    }
+    if (sn > 0)
+      by_type(keys.type, wide, [&](auto k, auto w) {
+        launch_group<decltype(k), decltype(w)::value>(d, src, sgrid, cnt, nullptr, nullptr, false, st, stream);
+      });
     device_exclusive_scan<int32_t, int32_t>(cnt, t->grp_off, nullptr, ngroups, tmp_buf.as<int64_t>(), stream);
     SJ_CUDA_TRY(cudaMemsetAsync(cnt, 0, (size_t)ngroups * sizeof(int32_t), stream));
-    if (n > 0) {
-      if (keys.type == SJ_INT32) {
-        if (wide) launch_group<int32_t, true>(d, keys, grid, cnt, t->grp_off, t->grp_rid, true, st, stream);
-        else launch_group<int32_t, false>(d, keys, grid, cnt, t->grp_off, t->grp_rid, true, st, stream);
-      } else {
-        if (wide) launch_group<int64_t, true>(d, keys, grid, cnt, t->grp_off, t->grp_rid, true, st, stream);
-        else launch_group<int64_t, false>(d, keys, grid, cnt, t->grp_off, t->grp_rid, true, st, stream);
-      }
-    }
+    if (sn > 0)
+      by_type(keys.type, wide, [&](auto k, auto w) {
+        launch_group<decltype(k), decltype(w)::value>(d, src, sgrid, cnt, t->grp_off, t->grp_rid, true, st, stream);
+      });
     if (cudaMemcpyAsync(&h, st, sizeof(h), cudaMemcpyDeviceToHost, stream) != cudaSuccess ||
         cudaStreamSynchronize(stream) != cudaSuccess)
       return fail(set_error(SJ_ERR_DEVICE, std::string("grouped build: ") + cudaGetErrorString(cudaGetLastError())));
@@ -490,6 +603,13 @@ sj_status destroy_table(sj_table* t, cudaStream_t stream) {
   if (t->slots) t->alloc.release(t->slots, t->slots_bytes, stream);
   if (t->grp_off) t->alloc.release(t->grp_off, t->grp_off_bytes, stream);
   if (t->grp_rid) t->alloc.release(t->grp_rid, t->grp_rid_bytes, stream);
+  if (t->arow) t->alloc.release(t->arow, t->arow_bytes, stream);
+  if (t->apay_owned) {
+    for (int c = 0; c < t->n_attached; ++c) {
+      if (t->apay[c]) t->alloc.release(t->apay[c], t->apay_bytes[c], stream);
+      if (t->apay_valid[c]) t->alloc.release(t->apay_valid[c], t->apay_valid_bytes[c], stream);
+    }
+  }
   delete t;
   return SJ_OK;
 }

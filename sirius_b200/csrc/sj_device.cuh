@@ -37,9 +37,11 @@ __host__ __device__ __forceinline__ uint64_t mix64(uint64_t x) {
 
 template <typename K>
 __host__ __device__ __forceinline__ uint64_t key_u64(K k);
+// Keys enter the hash sign-extended to 64 bits, so an int32 key and its (key - key_min) + key_min
+// reconstruction (the grouped build's shrink pass) hash identically.
 template <>
 __host__ __device__ __forceinline__ uint64_t key_u64<int32_t>(int32_t k) {
-  return (uint64_t)(uint32_t)k;
+  return (uint64_t)(int64_t)k;
 }
 template <>
 __host__ __device__ __forceinline__ uint64_t key_u64<int64_t>(int64_t k) {
@@ -75,23 +77,74 @@ struct Bucket {
   uint64_t a[4];  // PACKED64: 4 slots; WIDE128: {key0, rid0, key1, rid1}
 };
 
+// One bucket = one 32-byte sector. Read-only probes fetch it with a single 256-bit load
+// (ld.global.nc.v4.u64, sm_100); the build's insert pass reads it through L2 only (.cg) because
+// other threads are CASing the same slots.
 template <bool NC>
 __device__ __forceinline__ Bucket load_bucket(const void* slots, uint32_t b) {
-  const ulonglong2* p = reinterpret_cast<const ulonglong2*>(slots) + (size_t)b * 2;
-  ulonglong2 x, y;
-  if (NC) {
-    x = __ldg(p);
-    y = __ldg(p + 1);
-  } else {
-    x = __ldcg(p);
-    y = __ldcg(p + 1);
-  }
   Bucket r;
-  r.a[0] = x.x;
-  r.a[1] = x.y;
-  r.a[2] = y.x;
-  r.a[3] = y.y;
+  const unsigned long long* p = reinterpret_cast<const unsigned long long*>(slots) + (size_t)b * 4;
+  if (NC) {
+    asm("ld.global.nc.v4.u64 {%0, %1, %2, %3}, [%4];"
+        : "=l"(r.a[0]), "=l"(r.a[1]), "=l"(r.a[2]), "=l"(r.a[3])
+        : "l"(p));
+  } else {
+    const ulonglong2* q = reinterpret_cast<const ulonglong2*>(p);
+    const ulonglong2 x = __ldcg(q), y = __ldcg(q + 1);
+    r.a[0] = x.x;
+    r.a[1] = x.y;
+    r.a[2] = y.x;
+    r.a[3] = y.y;
+  }
   return r;
+}
+
+// A row-store record of up to 32 bytes in one load (4, 8, 16 or 32 bytes, naturally aligned).
+struct Record {
+  uint32_t w[8];
+};
+__device__ __forceinline__ Record load_record(const void* p, int bytes) {
+  Record r;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) r.w[k] = 0;
+  if (bytes == 32) {
+    asm("ld.global.nc.v8.u32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+        : "=r"(r.w[0]), "=r"(r.w[1]), "=r"(r.w[2]), "=r"(r.w[3]), "=r"(r.w[4]), "=r"(r.w[5]), "=r"(r.w[6]),
+          "=r"(r.w[7])
+        : "l"(p));
+  } else if (bytes == 16) {
+    const uint4 x = __ldg(reinterpret_cast<const uint4*>(p));
+    r.w[0] = x.x;
+    r.w[1] = x.y;
+    r.w[2] = x.z;
+    r.w[3] = x.w;
+  } else if (bytes == 8) {
+    const uint2 x = __ldg(reinterpret_cast<const uint2*>(p));
+    r.w[0] = x.x;
+    r.w[1] = x.y;
+  } else {
+    r.w[0] = __ldg(reinterpret_cast<const unsigned int*>(p));
+  }
+  return r;
+}
+// Field of `width` bytes at byte offset `off` (aligned to its width) of a record. `off` is the
+// same for every lane (a launch parameter), so the switch is a uniform branch.
+__device__ __forceinline__ uint64_t record_field(const Record& r, int off, int width) {
+  uint32_t lo = 0, hi = 0;
+  switch (off >> 2) {
+    case 0: lo = r.w[0]; hi = r.w[1]; break;
+    case 1: lo = r.w[1]; hi = r.w[2]; break;
+    case 2: lo = r.w[2]; hi = r.w[3]; break;
+    case 3: lo = r.w[3]; hi = r.w[4]; break;
+    case 4: lo = r.w[4]; hi = r.w[5]; break;
+    case 5: lo = r.w[5]; hi = r.w[6]; break;
+    case 6: lo = r.w[6]; hi = r.w[7]; break;
+    default: lo = r.w[7]; break;
+  }
+  if (width == 8) return ((uint64_t)hi << 32) | lo;
+  if (width == 4) return lo;
+  const uint32_t v = lo >> ((off & 3) * 8);
+  return width == 2 ? (v & 0xffffu) : (v & 0xffu);
 }
 
 template <bool WIDE>
@@ -107,6 +160,12 @@ struct SlotOps<false> {
   __device__ __forceinline__ static int32_t rid(const Bucket& bk, int q, uint32_t rbits) {
     return (int32_t)(bk.a[q] & ((1ull << rbits) - 1));
   }
+  // Probe form: ks = (key - key_min) << rid_bits, kmask = ~(row-id mask). One masked compare;
+  // EMPTY never matches because its key field is all ones and a live key field never is.
+  __device__ __forceinline__ static uint64_t probe_key(uint64_t kn, uint64_t, uint32_t rbits) { return kn << rbits; }
+  __device__ __forceinline__ static bool match_s(const Bucket& bk, int q, uint64_t ks, uint64_t kmask) {
+    return (bk.a[q] & kmask) == ks;
+  }
 };
 
 template <>
@@ -118,6 +177,10 @@ struct SlotOps<true> {
   }
   __device__ __forceinline__ static int32_t rid(const Bucket& bk, int q, uint32_t) {
     return (int32_t)bk.a[2 * q + 1];
+  }
+  __device__ __forceinline__ static uint64_t probe_key(uint64_t, uint64_t kb, uint32_t) { return kb; }
+  __device__ __forceinline__ static bool match_s(const Bucket& bk, int q, uint64_t kb, uint64_t) {
+    return bk.a[2 * q + 1] != kEmpty && bk.a[2 * q] == kb;
   }
 };
 
@@ -168,17 +231,32 @@ __device__ __forceinline__ unsigned long long warp_reserve(unsigned long long* c
 }
 
 // ---- payload gather --------------------------------------------------------------------------
+// A payload source: element i lives at data + i * stride (stride == width for a plain column,
+// the record size for the table's interleaved row store).
 struct PayloadIn {
   const void* data;
-  const uint32_t* valid;
+  const uint32_t* valid;   // cuDF bitmask (with voff), or NULL
+  const uint8_t* valid8;   // validity byte of element i at valid8 + i * vstride, or NULL
   int64_t voff;
   int32_t width;
+  int32_t stride;
+  int32_t vstride;
   int32_t pad;
 };
 struct PayloadOut {
   void* data;
   uint32_t* valid;
 };
+
+__host__ __device__ inline PayloadIn column_payload(const void* data, const uint32_t* valid, int64_t voff, int w) {
+  return PayloadIn{data, valid, nullptr, voff, w, w, 1, 0};
+}
+
+__device__ __forceinline__ bool has_validity(const PayloadIn& in) { return in.valid || in.valid8; }
+__device__ __forceinline__ bool payload_valid(const PayloadIn& in, int64_t i) {
+  if (in.valid8) return __ldg(in.valid8 + i * in.vstride) != 0;
+  return bit_valid(in.valid, in.voff, i);
+}
 
 struct GatherArgs {
   int32_t n_pin, n_bin;
@@ -190,6 +268,16 @@ struct GatherArgs {
   int32_t* out_brid;
   int64_t capacity;
   unsigned long long* d_count;
+  const int32_t* prid_map;  // probe array index -> probe row id (partitioned probe), or NULL
+  const int32_t* brid_map;  // build row id of table position p at brid_map + p * brid_stride bytes,
+  int32_t brid_stride;      //   or NULL when positions are the row ids
+  int32_t bin_by_pos;       // build payloads are the table's position-ordered attached copies
+  // The table's row store when the attached build payloads live in records of <= 32 bytes: one
+  // load per match returns the build row id and every attached field.
+  const void* rec;
+  int32_t rec_stride;
+  int16_t rec_off[kMaxPayload];   // byte offset of attached column c inside a record
+  int16_t rec_voff[kMaxPayload];  // byte offset of its validity byte, -1 when it has no NULLs
 };
 
 __device__ __forceinline__ uint64_t load_elem(const void* base, int64_t i, int w) {
@@ -215,6 +303,31 @@ __device__ __forceinline__ void store_elem_cs(void* base, int64_t i, int w, uint
     case 4: __stcs(reinterpret_cast<unsigned int*>(base) + i, (unsigned int)v); break;
     case 2: __stcs(reinterpret_cast<unsigned short*>(base) + i, (unsigned short)v); break;
     default: reinterpret_cast<unsigned char*>(base)[i] = (unsigned char)v; break;
+  }
+}
+
+// Strided payload element (plain column or interleaved record field).
+__device__ __forceinline__ uint64_t pl_load(const PayloadIn& in, int64_t i) {
+  const void* a = static_cast<const char*>(in.data) + i * in.stride;
+  switch (in.width) {
+    case 8: return __ldg(reinterpret_cast<const unsigned long long*>(a));
+    case 4: return __ldg(reinterpret_cast<const unsigned int*>(a));
+    case 2: return __ldg(reinterpret_cast<const unsigned short*>(a));
+    default: return __ldg(reinterpret_cast<const unsigned char*>(a));
+  }
+}
+__device__ __forceinline__ int32_t brid_of(const GatherArgs& g, int32_t pos) {
+  return g.brid_map ? __ldg(reinterpret_cast<const int32_t*>(reinterpret_cast<const char*>(g.brid_map) +
+                                                               (int64_t)pos * g.brid_stride))
+                    : pos;
+}
+
+__device__ __forceinline__ uint64_t load_elem_smem(const void* base, int64_t i, int w) {
+  switch (w) {
+    case 8: return reinterpret_cast<const unsigned long long*>(base)[i];
+    case 4: return reinterpret_cast<const unsigned int*>(base)[i];
+    case 2: return reinterpret_cast<const unsigned short*>(base)[i];
+    default: return reinterpret_cast<const unsigned char*>(base)[i];
   }
 }
 

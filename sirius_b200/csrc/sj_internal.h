@@ -66,6 +66,19 @@ struct Scratch {
   }
 };
 
+// ---- opt-in per-kernel timing (sj_timing_enable / sj_timing_collect) ---------------------------
+// While enabled, every KernelTimer scope records a CUDA event pair on its stream around the
+// launch it wraps; the calling thread collects the durations later. Off by default: no events.
+bool timing_enabled();
+struct KernelTimer {
+  KernelTimer(const char* name, cudaStream_t s);
+  ~KernelTimer();
+  KernelTimer(const KernelTimer&) = delete;
+  KernelTimer& operator=(const KernelTimer&) = delete;
+  int idx = -1;
+  cudaStream_t stream = nullptr;
+};
+
 int sm_count(int device);
 int type_width(int32_t t);  // bytes per element, 0 if invalid
 
@@ -90,8 +103,31 @@ struct sj_table {
   size_t slots_bytes = 0;
   int32_t* grp_off   = nullptr;  // GROUPED: #slots + 2 offsets (group #slots = NULL keys)
   size_t grp_off_bytes = 0;
-  int32_t* grp_rid   = nullptr;  // GROUPED: build row ids ordered by group
+  int32_t* grp_rid   = nullptr;  // GROUPED: table positions ordered by group
   size_t grp_rid_bytes = 0;
+  // Table positions. A slot's row-id field holds a position; the build row id of position p is
+  // the int32 at pos_rid + p * pos_stride bytes (pos_rid NULL: positions are the row ids). With
+  // radix partitioning positions follow partition order, so a partition's rows are contiguous.
+  int32_t* pos_rid   = nullptr;
+  int32_t pos_stride = 4;
+  // Row store, one record of arow_stride bytes (a power of two) per position:
+  //   [build row id (int32) | one validity byte per nullable attached column | attached payload
+  //    fields, each aligned to its width]
+  // so a match reads its row id and all its attached payloads from one record.
+  void* arow         = nullptr;
+  size_t arow_bytes  = 0;
+  int32_t arow_stride = 0;
+  // Attached build payload columns: field views into the row store, or (when positions are the
+  // row ids, i.e. NULLs are equal and the build has NULL keys) owned column copies.
+  int32_t n_attached = 0;
+  int32_t apay_type[8] = {};
+  void* apay[8]      = {};
+  int32_t apay_stride[8] = {};
+  uint8_t* apay_valid[8] = {};
+  int32_t apay_vstride[8] = {};
+  bool apay_owned    = false;
+  size_t apay_bytes[8] = {};
+  size_t apay_valid_bytes[8] = {};
   sj_join_params params{};
   int64_t num_slots() const;
 };
@@ -99,8 +135,8 @@ struct sj_table {
 namespace sj {
 
 // ---- kernel launchers (sj_build.cu / sj_probe.cu) ---------------------------------------------
-sj_status build_table(const sj_column& keys, const sj_join_params& p, const Allocator& alloc,
-                      cudaStream_t stream, sj_table** out);
+sj_status build_table(const sj_column& keys, const sj_column* payload, int32_t n_payload,
+                      const sj_join_params& p, const Allocator& alloc, cudaStream_t stream, sj_table** out);
 sj_status destroy_table(sj_table* t, cudaStream_t stream);
 
 struct GatherSpec {

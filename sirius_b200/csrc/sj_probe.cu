@@ -24,6 +24,7 @@
 
 #include "sj_device.cuh"
 #include "sj_internal.h"
+#include "sj_partition.cuh"
 #include "sj_scan.cuh"
 
 namespace sj {
@@ -79,14 +80,160 @@ __device__ __forceinline__ uint32_t live_rows(const TableDev& t, const K (&k)[KP
 }
 
 // ------------------------------------------------------------------------------------------------
+// Warp write-out. A warp stages its matches (probe row, build row id) in shared memory in
+// compacted order, reserves one output range with a single atomicAdd, and then writes every
+// output column with consecutive lanes on consecutive positions: full 32-byte sectors reach L2
+// instead of lane-strided partial ones, and the probe payload is read in near-sequential order.
+// ------------------------------------------------------------------------------------------------
+constexpr int kProbeThreads = 256;
+constexpr int kWarpsPerCta = kProbeThreads / 32;
+constexpr int kStage = 32 * KPT;  // matches one warp can stage per tile
+
+template <bool STREAM>
+__device__ __forceinline__ void emit_column(const PayloadIn& in, const PayloadOut& o, const int32_t* s_idx,
+                                            uint32_t tot, int64_t base, int64_t cap) {
+  const int lane = threadIdx.x & 31;
+  uint64_t v[KPT];
+#pragma unroll
+  for (int u = 0; u < KPT; ++u) {
+    const uint32_t i = lane + 32u * u;
+    v[u] = 0;
+    if (i < tot) v[u] = STREAM && in.stride == in.width ? load_elem_cs(in.data, s_idx[i], in.width) : pl_load(in, s_idx[i]);
+  }
+#pragma unroll
+  for (int u = 0; u < KPT; ++u) {
+    const uint32_t i = lane + 32u * u;
+    const int64_t p = base + i;
+    const bool live = i < tot && p < cap;
+    if (live) store_elem(o.data, p, in.width, v[u]);
+    if (has_validity(in)) {
+      const unsigned bits = __ballot_sync(kFullMask, live && payload_valid(in, s_idx[i]));
+      if (lane == 0 && bits) {
+        const int64_t p0 = base + 32u * u;
+        const int sh = (int)(p0 & 31);
+        atomicOr(o.valid + (p0 >> 5), bits << sh);
+        if (sh && (bits >> (32 - sh))) atomicOr(o.valid + (p0 >> 5) + 1, bits >> (32 - sh));
+      }
+    }
+  }
+}
+
+// s_row: probe array indices (row ids unless the probe was partitioned: prid_map).
+// s_rid: table positions (build row ids unless the table maps them: brid_map); rewritten in
+// place to build row ids after the position-ordered attached payloads have been gathered.
+// Row-store write-out: one record load per match gives the build row id and all attached fields.
+__device__ __forceinline__ void write_records(const Record (&r)[KPT / 2], int half, uint32_t tot, int64_t base,
+                                              const GatherArgs& g) {
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int h = 0; h < KPT / 2; ++h) {
+    const uint32_t i = lane + 32u * (half * (KPT / 2) + h);
+    const int64_t p = base + i;
+    const bool live = i < tot && p < g.capacity;
+    if (live && g.out_brid) g.out_brid[p] = (int32_t)r[h].w[0];
+    for (int c = 0; c < g.n_bin; ++c) {
+      const int w = g.bin[c].width;
+      if (live) store_elem(g.bout[c].data, p, w, record_field(r[h], g.rec_off[c], w));
+      if (g.rec_voff[c] >= 0) {
+        const unsigned bits = __ballot_sync(kFullMask, live && record_field(r[h], g.rec_voff[c], 1) != 0);
+        if (lane == 0 && bits) {
+          const int64_t p0 = base + 32u * (half * (KPT / 2) + h);
+          const int sh = (int)(p0 & 31);
+          atomicOr(g.bout[c].valid + (p0 >> 5), bits << sh);
+          if (sh && (bits >> (32 - sh))) atomicOr(g.bout[c].valid + (p0 >> 5) + 1, bits >> (32 - sh));
+        }
+      }
+    }
+  }
+}
+
+__device__ __forceinline__ void load_records(Record (&r)[KPT / 2], int half, const int32_t* s_rid, uint32_t tot,
+                                             const GatherArgs& g) {
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int h = 0; h < KPT / 2; ++h) {
+    const uint32_t i = lane + 32u * (half * (KPT / 2) + h);
+    if (i < tot)
+      r[h] = load_record(static_cast<const char*>(g.rec) + (int64_t)s_rid[i] * g.rec_stride, g.rec_stride);
+  }
+}
+
+// s_row: probe array indices (row ids unless the probe was partitioned: prid_map).
+// s_rid: table positions (build row ids unless the table maps them: brid_map); rewritten in
+// place to build row ids after the position-ordered attached payloads have been gathered.
+// base: the warp's first output position; when `deferred` it is lane 0's still-pending atomicAdd
+// result, broadcast only after this warp's gather loads are in flight.
+__device__ __forceinline__ void warp_write_out(const int32_t* s_row, int32_t* s_rid, uint32_t tot,
+                                               unsigned long long base_in, bool deferred, const GatherArgs& g) {
+  const int lane = threadIdx.x & 31;
+  if (g.rec) {
+    int32_t pr[KPT];
+#pragma unroll
+    for (int u = 0; u < KPT; ++u) {
+      const uint32_t i = lane + 32u * u;
+      pr[u] = 0;
+      if (i < tot) pr[u] = g.prid_map ? __ldg(g.prid_map + s_row[i]) : s_row[i];
+    }
+    Record r[KPT / 2];
+    load_records(r, 0, s_rid, tot, g);
+    const int64_t base = (int64_t)(deferred ? __shfl_sync(kFullMask, base_in, 0) : base_in);
+    if (g.out_prid) {
+#pragma unroll
+      for (int u = 0; u < KPT; ++u) {
+        const uint32_t i = lane + 32u * u;
+        const int64_t p = base + i;
+        if (i < tot && p < g.capacity) g.out_prid[p] = pr[u];
+      }
+    }
+    write_records(r, 0, tot, base, g);
+    load_records(r, 1, s_rid, tot, g);
+    write_records(r, 1, tot, base, g);
+    for (int c = 0; c < g.n_pin; ++c) emit_column<true>(g.pin[c], g.pout[c], s_row, tot, base, g.capacity);
+    return;
+  }
+  const int64_t base = (int64_t)(deferred ? __shfl_sync(kFullMask, base_in, 0) : base_in);
+  if (g.out_prid) {
+    for (uint32_t i = lane; i < tot; i += 32) {
+      const int64_t p = base + i;
+      if (p < g.capacity) g.out_prid[p] = g.prid_map ? __ldg(g.prid_map + s_row[i]) : s_row[i];
+    }
+  }
+  if (g.bin_by_pos)
+    for (int c = 0; c < g.n_bin; ++c) emit_column<false>(g.bin[c], g.bout[c], s_rid, tot, base, g.capacity);
+  if (g.brid_map) {
+    for (uint32_t i = lane; i < tot; i += 32) s_rid[i] = brid_of(g, s_rid[i]);
+    __syncwarp();
+  }
+  if (g.out_brid) {
+    for (uint32_t i = lane; i < tot; i += 32) {
+      const int64_t p = base + i;
+      if (p < g.capacity) g.out_brid[p] = s_rid[i];
+    }
+  }
+  if (!g.bin_by_pos)
+    for (int c = 0; c < g.n_bin; ++c) emit_column<false>(g.bin[c], g.bout[c], s_rid, tot, base, g.capacity);
+  for (int c = 0; c < g.n_pin; ++c) emit_column<true>(g.pin[c], g.pout[c], s_row, tot, base, g.capacity);
+}
+
+// ------------------------------------------------------------------------------------------------
 // DISTINCT: probe + gather in one pass
 // ------------------------------------------------------------------------------------------------
-template <typename K, bool WIDE, bool VEC, bool COUNT_ONLY>
-__global__ void __launch_bounds__(256) probe_distinct_kernel(TableDev t, const K* __restrict__ keys,
-                                                             const uint32_t* __restrict__ kv, int64_t kvoff,
-                                                             int64_t n, GatherArgs g) {
+// CTA_AGG: the CTA sums its warps' match counts and reserves the whole tile's output range with
+// one atomicAdd (instead of one per warp), which matters when a probe of tens of millions of rows
+// would otherwise queue ~10^5-10^6 atomics on the single output counter.
+template <typename K, bool WIDE, bool VEC, bool COUNT_ONLY, bool CTA_AGG>
+__global__ void __launch_bounds__(kProbeThreads, 4) probe_distinct_kernel(TableDev t, const K* __restrict__ keys,
+                                                                           const uint32_t* __restrict__ kv,
+                                                                           int64_t kvoff, int64_t n_host,
+                                                                           const int64_t* d_n, GatherArgs g) {
   using Ops = SlotOps<WIDE>;
+  __shared__ int32_t s_row[kWarpsPerCta][kStage];
+  __shared__ int32_t s_rid[kWarpsPerCta][kStage];
+  __shared__ unsigned s_wtot[kWarpsPerCta], s_wbase[kWarpsPerCta];
+  __shared__ unsigned long long s_cta_base;
   const int lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
+  const int64_t n = d_n ? *d_n : n_host;
   const int64_t per_cta = (int64_t)blockDim.x * KPT;
   const int64_t tiles = (n + per_cta - 1) / per_cta;
   unsigned long long counted = 0;
@@ -96,13 +243,15 @@ __global__ void __launch_bounds__(256) probe_distinct_kernel(TableDev t, const K
     load_keys<K>(keys, row0, n, VEC, k);
     uint32_t act = live_rows<K>(t, k, row0, n, kv, kvoff);
     uint32_t b[KPT];
-    uint64_t kn[KPT];
+    uint64_t ks[KPT];
+    const uint64_t kmask = ~((1ull << t.rbits) - 1);
 #pragma unroll
     for (int j = 0; j < KPT; ++j) {
-      b[j] = home_bucket(t, key_u64<K>(k[j]));
-      kn[j] = (uint64_t)(long long)k[j] - (uint64_t)t.kmin;
+      const uint64_t kb = key_u64<K>(k[j]);
+      b[j] = home_bucket(t, kb);
+      ks[j] = Ops::probe_key((uint64_t)(long long)k[j] - (uint64_t)t.kmin, kb, t.rbits);
     }
-    int32_t rid[KPT];
+    int32_t rid[KPT] = {0, 0, 0, 0};
     uint32_t hit = 0;
     for (uint32_t step = 0; act && step <= t.segmask; ++step) {
       Bucket bk[KPT];
@@ -115,7 +264,7 @@ __global__ void __launch_bounds__(256) probe_distinct_kernel(TableDev t, const K
         bool done = false;
 #pragma unroll
         for (int q = 0; q < Ops::kSlots; ++q) {
-          if (!done && Ops::match(bk[j], q, kn[j], key_u64<K>(k[j]), t.rbits)) {
+          if (!done && Ops::match_s(bk[j], q, ks[j], kmask)) {
             rid[j] = Ops::rid(bk[j], q, t.rbits);
             hit |= 1u << j;
             done = true;
@@ -131,47 +280,44 @@ __global__ void __launch_bounds__(256) probe_distinct_kernel(TableDev t, const K
       counted += cnt;
       continue;
     }
-    const unsigned long long pos0 = warp_reserve(g.d_count, cnt);
-    int64_t pos[KPT];
-#pragma unroll
-    for (int j = 0; j < KPT; ++j) pos[j] = (int64_t)pos0 + __popc(hit & ((1u << j) - 1));
+    const uint32_t incl = warp_inclusive_sum(cnt);
+    const uint32_t tot = __shfl_sync(kFullMask, incl, 31);
+    if (!CTA_AGG && tot == 0) continue;
+    unsigned long long early = 0;
+    if (!CTA_AGG && lane == 0) early = atomicAdd(g.d_count, (unsigned long long)tot);
+    uint32_t sp = incl - cnt;
 #pragma unroll
     for (int j = 0; j < KPT; ++j) {
-      if ((hit >> j & 1u) && pos[j] < g.capacity) {
-        if (g.out_prid) __stcs(g.out_prid + pos[j], (int)(row0 + j));
-        if (g.out_brid) __stcs(g.out_brid + pos[j], (int)rid[j]);
+      if (hit >> j & 1u) {
+        s_row[warp][sp] = (int32_t)(row0 + j);
+        s_rid[warp][sp] = rid[j];
+        ++sp;
       }
     }
-    for (int c = 0; c < g.n_pin; ++c) {
-      const PayloadIn in = g.pin[c];
-      const PayloadOut o = g.pout[c];
-      uint64_t v[KPT];
+    unsigned long long base = 0;
+    bool deferred = false;
+    if (CTA_AGG) {
+      if (lane == 0) s_wtot[warp] = tot;
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        unsigned run = 0;
 #pragma unroll
-      for (int j = 0; j < KPT; ++j)
-        if (hit >> j & 1u) v[j] = load_elem_cs(in.data, row0 + j, in.width);
-#pragma unroll
-      for (int j = 0; j < KPT; ++j) {
-        if ((hit >> j & 1u) && pos[j] < g.capacity) {
-          store_elem_cs(o.data, pos[j], in.width, v[j]);
-          if (in.valid && bit_valid(in.valid, in.voff, row0 + j)) set_out_bit(o.valid, pos[j]);
+        for (int w = 0; w < kWarpsPerCta; ++w) {
+          s_wbase[w] = run;
+          run += s_wtot[w];
         }
+        s_cta_base = run ? atomicAdd(g.d_count, (unsigned long long)run) : 0ull;
       }
+      __syncthreads();
+      base = s_cta_base + s_wbase[warp];
+    } else {
+      // lane 0's atomic result is only consumed by the stores, after the gather loads are issued
+      base = early;
+      deferred = true;
+      __syncwarp();
     }
-    for (int c = 0; c < g.n_bin; ++c) {
-      const PayloadIn in = g.bin[c];
-      const PayloadOut o = g.bout[c];
-      uint64_t v[KPT];
-#pragma unroll
-      for (int j = 0; j < KPT; ++j)
-        if (hit >> j & 1u) v[j] = load_elem(in.data, rid[j], in.width);
-#pragma unroll
-      for (int j = 0; j < KPT; ++j) {
-        if ((hit >> j & 1u) && pos[j] < g.capacity) {
-          store_elem_cs(o.data, pos[j], in.width, v[j]);
-          if (in.valid && bit_valid(in.valid, in.voff, rid[j])) set_out_bit(o.valid, pos[j]);
-        }
-      }
-    }
+    if (tot) warp_write_out(s_row[warp], s_rid[warp], tot, base, deferred, g);
+    __syncwarp();
   }
   if (COUNT_ONLY) {
 #pragma unroll
@@ -184,13 +330,16 @@ __global__ void __launch_bounds__(256) probe_distinct_kernel(TableDev t, const K
 // GROUPED pass A: find each probe row's group; compact (row, start, size); sum the output size.
 // ------------------------------------------------------------------------------------------------
 template <typename K, bool WIDE, bool VEC, bool COMPACT>
-__global__ void __launch_bounds__(256) grouped_match_kernel(TableDev t, const K* __restrict__ keys,
-                                                            const uint32_t* __restrict__ kv, int64_t kvoff,
-                                                            int64_t n, int32_t* m_row, int32_t* m_start,
-                                                            int32_t* m_cnt, unsigned long long* d_nent,
-                                                            unsigned long long* d_total) {
+__global__ void __launch_bounds__(kProbeThreads, 4) grouped_match_kernel(TableDev t, const K* __restrict__ keys,
+                                                                          const uint32_t* __restrict__ kv,
+                                                                          int64_t kvoff, int64_t n, int32_t* m_row,
+                                                                          int32_t* m_start, int32_t* m_cnt,
+                                                                          unsigned long long* d_nent,
+                                                                          unsigned long long* d_total) {
   using Ops = SlotOps<WIDE>;
+  __shared__ int32_t s_e[kWarpsPerCta][3][kStage];
   const int lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
   const int64_t per_cta = (int64_t)blockDim.x * KPT;
   const int64_t tiles = (n + per_cta - 1) / per_cta;
   unsigned long long total = 0;
@@ -201,12 +350,14 @@ __global__ void __launch_bounds__(256) grouped_match_kernel(TableDev t, const K*
     uint32_t act = live_rows<K>(t, k, row0, n, kv, kvoff);
     int32_t slot[KPT];
     uint32_t b[KPT];
-    uint64_t kn[KPT];
+    uint64_t ks[KPT];
+    const uint64_t kmask = ~((1ull << t.rbits) - 1);
 #pragma unroll
     for (int j = 0; j < KPT; ++j) {
       slot[j] = -1;
-      b[j] = home_bucket(t, key_u64<K>(k[j]));
-      kn[j] = (uint64_t)(long long)k[j] - (uint64_t)t.kmin;
+      const uint64_t kb = key_u64<K>(k[j]);
+      b[j] = home_bucket(t, kb);
+      ks[j] = Ops::probe_key((uint64_t)(long long)k[j] - (uint64_t)t.kmin, kb, t.rbits);
       if (t.null_group >= 0 && row0 + j < n && !bit_valid(kv, kvoff, row0 + j)) slot[j] = t.null_group;
     }
     for (uint32_t step = 0; act && step <= t.segmask; ++step) {
@@ -220,7 +371,7 @@ __global__ void __launch_bounds__(256) grouped_match_kernel(TableDev t, const K*
         bool done = false;
 #pragma unroll
         for (int q = 0; q < Ops::kSlots; ++q) {
-          if (!done && Ops::match(bk[j], q, kn[j], key_u64<K>(k[j]), t.rbits)) {
+          if (!done && Ops::match_s(bk[j], q, ks[j], kmask)) {
             slot[j] = (int32_t)(b[j] * Ops::kSlots + q);
             done = true;
           }
@@ -243,15 +394,31 @@ __global__ void __launch_bounds__(256) grouped_match_kernel(TableDev t, const K*
       }
     }
     if (COMPACT) {
-      const unsigned long long p0 = warp_reserve(d_nent, __popc(hit));
+      // stage (row, start, size) in compacted order, then write the warp's range coalesced
+      const uint32_t c = __popc(hit);
+      const uint32_t incl = warp_inclusive_sum(c);
+      const uint32_t tot = __shfl_sync(kFullMask, incl, 31);
+      if (tot) {
+        unsigned long long base = 0;
+        if (lane == 0) base = atomicAdd(d_nent, (unsigned long long)tot);
+        base = __shfl_sync(kFullMask, base, 0);
+        uint32_t sp = incl - c;
 #pragma unroll
-      for (int j = 0; j < KPT; ++j) {
-        if (hit >> j & 1u) {
-          const int64_t p = (int64_t)p0 + __popc(hit & ((1u << j) - 1));
-          m_row[p] = (int32_t)(row0 + j);
-          m_start[p] = start[j];
-          m_cnt[p] = cnt[j];
+        for (int j = 0; j < KPT; ++j) {
+          if (hit >> j & 1u) {
+            s_e[warp][0][sp] = (int32_t)(row0 + j);
+            s_e[warp][1][sp] = start[j];
+            s_e[warp][2][sp] = cnt[j];
+            ++sp;
+          }
         }
+        __syncwarp();
+        for (uint32_t i = lane; i < tot; i += 32) {
+          m_row[base + i] = s_e[warp][0][i];
+          m_start[base + i] = s_e[warp][1][i];
+          m_cnt[base + i] = s_e[warp][2][i];
+        }
+        __syncwarp();
       }
     }
   }
@@ -314,11 +481,12 @@ __global__ void __launch_bounds__(kExpandThreads) expand_kernel(const int32_t* _
     for (int m = 0; m < kExpandItems; ++m) {
       const int64_t j = j0 + (int64_t)m * kExpandThreads + threadIdx.x;
       const bool live = j < j1;
-      int32_t row = 0, rid = 0;
+      int32_t row = 0, pos = 0, rid = 0;
       if (live) {
         const int64_t e = upper_index(s_off, 0, ne - 1, j);
         row = s_row[e];
-        rid = __ldg(grp_rid + s_start[e] + (j - s_off[e]));
+        pos = __ldg(grp_rid + s_start[e] + (j - s_off[e]));
+        rid = brid_of(g, pos);
         if (g.out_prid) __stcs(g.out_prid + j, row);
         if (g.out_brid) __stcs(g.out_brid + j, rid);
       }
@@ -326,22 +494,23 @@ __global__ void __launch_bounds__(kExpandThreads) expand_kernel(const int32_t* _
         const PayloadIn in = g.pin[c];
         bool v = false;
         if (live) {
-          store_elem_cs(g.pout[c].data, j, in.width, load_elem(in.data, row, in.width));
-          v = bit_valid(in.valid, in.voff, row);
+          store_elem_cs(g.pout[c].data, j, in.width, pl_load(in, row));
+          v = payload_valid(in, row);
         }
-        if (in.valid) {
+        if (has_validity(in)) {
           const unsigned word = __ballot_sync(kFullMask, v);
           if (lane == 0 && j - lane < j1) g.pout[c].valid[(j - lane) >> 5] = word;
         }
       }
       for (int c = 0; c < g.n_bin; ++c) {
         const PayloadIn in = g.bin[c];
+        const int32_t idx = g.bin_by_pos ? pos : rid;
         bool v = false;
         if (live) {
-          store_elem_cs(g.bout[c].data, j, in.width, load_elem(in.data, rid, in.width));
-          v = bit_valid(in.valid, in.voff, rid);
+          store_elem_cs(g.bout[c].data, j, in.width, pl_load(in, idx));
+          v = payload_valid(in, idx);
         }
-        if (in.valid) {
+        if (has_validity(in)) {
           const unsigned word = __ballot_sync(kFullMask, v);
           if (lane == 0 && j - lane < j1) g.bout[c].valid[(j - lane) >> 5] = word;
         }
@@ -366,33 +535,44 @@ static int probe_grid(const sj_table* t, int64_t n, int block) {
 }
 
 template <typename K, bool WIDE, bool VEC, bool COUNT_ONLY>
-static void launch_distinct(const sj_table* t, const sj_column& p, const GatherArgs& g, cudaStream_t s) {
-  const int block = 256;
-  probe_distinct_kernel<K, WIDE, VEC, COUNT_ONLY><<<probe_grid(t, p.num_rows, block), block, 0, s>>>(
-      table_dev(t), static_cast<const K*>(p.data), p.validity, p.validity_offset, p.num_rows, g);
+static void launch_distinct(const sj_table* t, const sj_column& p, const int64_t* d_n, const GatherArgs& g,
+                            cudaStream_t s) {
+  const int block = kProbeThreads;
+  const int grid = probe_grid(t, p.num_rows, block);
+  // output reservation: per CTA tile for large probes (or when asked), per warp otherwise
+  const int agg = t->params.aggregation;
+  const bool cta = agg == SJ_AGG_CTA || (agg == SJ_AGG_AUTO && p.num_rows >= (1 << 20));
+  KernelTimer timer(COUNT_ONLY ? "probe_distinct_count" : "probe_distinct", s);
+  if (cta && !COUNT_ONLY)
+    probe_distinct_kernel<K, WIDE, VEC, COUNT_ONLY, true><<<grid, block, 0, s>>>(
+        table_dev(t), static_cast<const K*>(p.data), p.validity, p.validity_offset, p.num_rows, d_n, g);
+  else
+    probe_distinct_kernel<K, WIDE, VEC, COUNT_ONLY, false><<<grid, block, 0, s>>>(
+        table_dev(t), static_cast<const K*>(p.data), p.validity, p.validity_offset, p.num_rows, d_n, g);
 }
 
+// d_n: optional device-resident row count (a partitioned probe's valid rows); p.num_rows bounds it.
 template <bool COUNT_ONLY>
-static void dispatch_distinct(const sj_table* t, const sj_column& p, const GatherArgs& g, cudaStream_t s) {
+static void dispatch_distinct(const sj_table* t, const sj_column& p, const int64_t* d_n, const GatherArgs& g,
+                              cudaStream_t s) {
   const bool wide = t->slot_kind == SJ_SLOT_WIDE128;
   const bool vec = aligned16(p.data);
+#define SJ_D(K, W, V) launch_distinct<K, W, V, COUNT_ONLY>(t, p, d_n, g, s)
   if (t->key_type == SJ_INT32) {
-    if (wide) vec ? launch_distinct<int32_t, true, true, COUNT_ONLY>(t, p, g, s)
-                  : launch_distinct<int32_t, true, false, COUNT_ONLY>(t, p, g, s);
-    else vec ? launch_distinct<int32_t, false, true, COUNT_ONLY>(t, p, g, s)
-             : launch_distinct<int32_t, false, false, COUNT_ONLY>(t, p, g, s);
+    if (wide) { if (vec) SJ_D(int32_t, true, true); else SJ_D(int32_t, true, false); }
+    else { if (vec) SJ_D(int32_t, false, true); else SJ_D(int32_t, false, false); }
   } else {
-    if (wide) vec ? launch_distinct<int64_t, true, true, COUNT_ONLY>(t, p, g, s)
-                  : launch_distinct<int64_t, true, false, COUNT_ONLY>(t, p, g, s);
-    else vec ? launch_distinct<int64_t, false, true, COUNT_ONLY>(t, p, g, s)
-             : launch_distinct<int64_t, false, false, COUNT_ONLY>(t, p, g, s);
+    if (wide) { if (vec) SJ_D(int64_t, true, true); else SJ_D(int64_t, true, false); }
+    else { if (vec) SJ_D(int64_t, false, true); else SJ_D(int64_t, false, false); }
   }
+#undef SJ_D
 }
 
 template <typename K, bool WIDE, bool VEC, bool COMPACT>
 static void launch_match(const sj_table* t, const sj_column& p, int32_t* m_row, int32_t* m_start, int32_t* m_cnt,
                          unsigned long long* d_nent, unsigned long long* d_total, cudaStream_t s) {
-  const int block = 256;
+  const int block = kProbeThreads;
+  KernelTimer timer(COMPACT ? "grouped_match" : "grouped_count", s);
   grouped_match_kernel<K, WIDE, VEC, COMPACT><<<probe_grid(t, p.num_rows, block), block, 0, s>>>(
       table_dev(t), static_cast<const K*>(p.data), p.validity, p.validity_offset, p.num_rows, m_row, m_start,
       m_cnt, d_nent, d_total);
@@ -431,7 +611,7 @@ sj_status probe_count(const sj_table* t, const sj_column& p, const Allocator& al
   if (t->layout == SJ_LAYOUT_DISTINCT) {
     GatherArgs g{};
     g.d_count = dc;
-    dispatch_distinct<true>(t, p, g, s);
+    dispatch_distinct<true>(t, p, nullptr, g, s);
   } else {
     dispatch_match<false>(t, p, nullptr, nullptr, nullptr, nullptr, dc, s);
   }
@@ -445,8 +625,12 @@ static sj_status fill_gather(const sj_table* t, const sj_column& p, const Gather
     return set_error(SJ_ERR_INVALID, "at most 8 payload columns per side");
   if (gs.capacity < 0) return set_error(SJ_ERR_INVALID, "capacity must be >= 0");
   if ((gs.n_probe_payload && (!gs.probe_payload || !gs.out_probe_payload)) ||
-      (gs.n_build_payload && (!gs.build_payload || !gs.out_build_payload)))
+      (gs.n_build_payload && !gs.out_build_payload))
     return set_error(SJ_ERR_INVALID, "payload column arrays must not be NULL");
+  const bool attached = gs.n_build_payload > 0 && gs.build_payload == nullptr;
+  if (attached && gs.n_build_payload != t->n_attached)
+    return set_error(SJ_ERR_INVALID, "build_payload is NULL (use the attached columns) but num_build_payload "
+                                     "differs from the number of columns attached at build");
   g.n_pin = gs.n_probe_payload;
   g.n_bin = gs.n_build_payload;
   auto fill = [&](const sj_column& in, const sj_mut_column& out, int64_t rows, PayloadIn& pi, PayloadOut& po,
@@ -458,23 +642,109 @@ static sj_status fill_gather(const sj_table* t, const sj_column& p, const Gather
     if (gs.capacity > 0 && !out.data) return set_error(SJ_ERR_INVALID, std::string(side) + " output data is NULL");
     if (in.validity && gs.capacity > 0 && !out.validity)
       return set_error(SJ_ERR_INVALID, std::string(side) + " payload has NULLs but its output has no validity");
-    pi.data = in.data;
-    pi.valid = in.validity;
-    pi.voff = in.validity_offset;
-    pi.width = type_width(in.type);
+    pi = column_payload(in.data, in.validity, in.validity_offset, type_width(in.type));
     po.data = out.data;
     po.valid = in.validity ? out.validity : nullptr;
     return SJ_OK;
   };
   for (int c = 0; c < g.n_pin; ++c)
     SJ_TRY(fill(gs.probe_payload[c], gs.out_probe_payload[c], p.num_rows, g.pin[c], g.pout[c], "probe"));
-  for (int c = 0; c < g.n_bin; ++c)
-    SJ_TRY(fill(gs.build_payload[c], gs.out_build_payload[c], t->build_rows, g.bin[c], g.bout[c], "build"));
+  if (attached) {
+    for (int c = 0; c < g.n_bin; ++c) {
+      const sj_mut_column& out = gs.out_build_payload[c];
+      if (out.type != t->apay_type[c]) return set_error(SJ_ERR_INVALID, "attached build output type differs");
+      if (gs.capacity > 0 && !out.data) return set_error(SJ_ERR_INVALID, "build output data is NULL");
+      if (t->apay_valid[c] && gs.capacity > 0 && !out.validity)
+        return set_error(SJ_ERR_INVALID, "attached build payload has NULLs but its output has no validity");
+      g.bin[c] = PayloadIn{t->apay[c], nullptr, t->apay_valid[c], 0, type_width(t->apay_type[c]), t->apay_stride[c],
+                           t->apay_vstride[c], 0};
+      g.bout[c] = PayloadOut{out.data, t->apay_valid[c] ? out.validity : nullptr};
+      if (t->arow) {
+        g.rec_off[c] = (int16_t)(static_cast<const char*>(t->apay[c]) - static_cast<const char*>(t->arow));
+        g.rec_voff[c] = t->apay_valid[c] ? (int16_t)(reinterpret_cast<const char*>(t->apay_valid[c]) -
+                                                     static_cast<const char*>(t->arow))
+                                         : (int16_t)-1;
+      }
+    }
+    g.bin_by_pos = 1;
+    if (t->arow && t->arow_stride <= 32) {
+      g.rec = t->arow;
+      g.rec_stride = t->arow_stride;
+    }
+  } else {
+    for (int c = 0; c < g.n_bin; ++c)
+      SJ_TRY(fill(gs.build_payload[c], gs.out_build_payload[c], t->build_rows, g.bin[c], g.bout[c], "build"));
+  }
+  g.brid_map = t->pos_rid;
+  g.brid_stride = t->pos_stride;
   g.out_prid = gs.out_probe_rid;
   g.out_brid = gs.out_build_rid;
   g.capacity = gs.capacity;
   return SJ_OK;
 }
+
+static size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
+
+// Partitioned probe of a DISTINCT table: radix-scatter the probe rows (key, row id, payloads) by
+// the table's partition bits, then stream the partitioned arrays through the probe kernel, so
+// each partition's probes hit its L2-resident table segment and attached payload rows.
+// Probe-side radix bits: the coarsest prefix of the table's partition bits whose share of the
+// table footprint (slots + position map + attached payloads) stays under ~40 MB of L2. A coarse
+// probe partition covers 2^(table bits - probe bits) contiguous table segments, and fewer
+// partitions mean longer contiguous runs in the scatter.
+static int probe_partition_bits(const sj_table* t) {
+  size_t fp = t->slots_bytes + t->arow_bytes;
+  const size_t kShare = 40ull << 20;
+  int b = 1;
+  while (b < t->pbits && (fp >> b) > kShare) ++b;
+  return std::min(b, t->pbits);
+}
+
+static sj_status probe_partitioned(const sj_table* t, const sj_column& p, GatherArgs g, const Allocator& alloc,
+                                   cudaStream_t s) {
+  const int64_t n = p.num_rows;
+  const int pbits = probe_partition_bits(t);
+  const int kw = t->key_type == SJ_INT32 ? 4 : 8;
+  size_t bytes = align256((size_t)n * kw) + align256((size_t)n * 4) + partition_scratch_bytes(pbits, t->device);
+  for (int c = 0; c < g.n_pin; ++c)
+    bytes += align256((size_t)n * g.pin[c].width) + (g.pin[c].valid ? align256((size_t)n) : 0);
+  Scratch sc;
+  SJ_TRY(sc.get(alloc, bytes, s));
+  char* cur = sc.as<char>();
+  auto carve = [&](size_t b) {
+    char* r = cur;
+    cur += align256(b);
+    return r;
+  };
+  PartSrc ps{};
+  PartDst pd{};
+  ps.keys = p.data;
+  ps.kvalid = p.validity;
+  ps.kvoff = p.validity_offset;
+  ps.n = n;
+  ps.n_pay = g.n_pin;
+  pd.keys = carve((size_t)n * kw);
+  pd.rid = reinterpret_cast<int32_t*>(carve((size_t)n * 4));
+  for (int c = 0; c < g.n_pin; ++c) {
+    ps.pay[c] = g.pin[c];
+    pd.pay[c] = carve((size_t)n * g.pin[c].width);
+    pd.valid8[c] = g.pin[c].valid ? reinterpret_cast<uint8_t*>(carve((size_t)n)) : nullptr;
+  }
+  void* pscratch = carve(partition_scratch_bytes(pbits, t->device));
+  const int64_t *d_total, *d_offs;
+  int G;
+  SJ_TRY(radix_partition(ps, t->key_type, pbits, pd, pscratch, t->device, s, &d_total, &d_offs, &G));
+  g.prid_map = pd.rid;
+  for (int c = 0; c < g.n_pin; ++c)
+    g.pin[c] = PayloadIn{pd.pay[c], nullptr, pd.valid8[c], 0, g.pin[c].width, g.pin[c].width, 1, 0};
+  const sj_column pk{pd.keys, nullptr, 0, n, t->key_type, 0};
+  dispatch_distinct<false>(t, pk, d_total, g, s);
+  SJ_CUDA_TRY(cudaGetLastError());
+  return SJ_OK;
+}
+
+// Probes of at least this many rows into a partitioned table take the partitioned path.
+constexpr int64_t kMinPartitionedProbe = 1 << 16;
 
 sj_status probe_gather(const sj_table* t, const sj_column& p, const GatherSpec& gs, const Allocator& alloc,
                        cudaStream_t s, int64_t* d_count) {
@@ -491,7 +761,8 @@ sj_status probe_gather(const sj_table* t, const sj_column& p, const GatherSpec& 
   if (p.num_rows == 0) return SJ_OK;
 
   if (t->layout == SJ_LAYOUT_DISTINCT) {
-    dispatch_distinct<false>(t, p, g, s);
+    if (t->pbits > 0 && p.num_rows >= kMinPartitionedProbe) return probe_partitioned(t, p, g, alloc, s);
+    dispatch_distinct<false>(t, p, nullptr, g, s);
     SJ_CUDA_TRY(cudaGetLastError());
     return SJ_OK;
   }
@@ -510,8 +781,12 @@ sj_status probe_gather(const sj_table* t, const sj_column& p, const GatherSpec& 
   unsigned long long* d_nent = reinterpret_cast<unsigned long long*>(base + 3 * b_row + b_off + b_tmp);
   SJ_CUDA_TRY(cudaMemsetAsync(d_nent, 0, sizeof(unsigned long long), s));
   dispatch_match<true>(t, p, m_row, m_start, m_cnt, d_nent, g.d_count, s);
-  device_exclusive_scan<int32_t, int64_t>(m_cnt, m_off, d_nent, 0, tmp, s);
+  {
+    KernelTimer timer("scan", s);
+    device_exclusive_scan<int32_t, int64_t>(m_cnt, m_off, d_nent, 0, tmp, s);
+  }
   const int grid = sm_count(t->device) * 4;
+  KernelTimer timer("expand", s);
   expand_kernel<<<grid, kExpandThreads, 0, s>>>(m_row, m_start, m_off, d_nent, t->grp_rid, g);
   SJ_CUDA_TRY(cudaGetLastError());
   return SJ_OK;

@@ -92,7 +92,7 @@ __global__ void __launch_bounds__(kScanThreads) scan_down_kernel(const Tin* __re
     int64_t tot;
     const int64_t ex = block_exclusive_sum<kScanThreads>(v, s_warp, tot);
     if (i < hi) out[i] = (Tout)(run + ex);
-    if (i == n - 1) out[n] = (Tout)(run + ex + v);  // the total
+    if (i < hi && i == n - 1) out[n] = (Tout)(run + ex + v);  // the total
     run += tot;
   }
 }

@@ -123,20 +123,32 @@ class HashTable:
     """A built table resident on the device (one partition slot of the BUILD_PROBE mode)."""
 
     def __init__(self, keys: torch.Tensor, validity: Optional[torch.Tensor] = None, *,
-                 layout: int = L.SJ_LAYOUT_AUTO, null_equality: int = L.SJ_NULLS_UNEQUAL,
+                 attach=(), layout: int = L.SJ_LAYOUT_AUTO, null_equality: int = L.SJ_NULLS_UNEQUAL,
                  load_factor: float = 0.5, partition_bits: int = 0, force_wide: bool = False,
-                 ctas_per_sm: int = 0, stream: Optional[torch.cuda.Stream] = None):
+                 ctas_per_sm: int = 0, aggregation: int = L.SJ_AGG_AUTO,
+                 stream: Optional[torch.cuda.Stream] = None):
+        """Build the table. ``attach``: build payload columns (tensor or (tensor, validity)) the
+        table copies in its own position order (sj_build_ex); gather them with
+        ``probe_gather(..., attached=True)``. ``partition_bits``: 0 = automatic, -1 = never."""
         self._lib = L.load()
         self._handle = ctypes.c_void_p()
         self.keys = keys
         self.params = L.default_params(layout=layout, null_equality=null_equality, load_factor=load_factor,
-                                       partition_bits=partition_bits, force_wide=int(force_wide))
+                                       partition_bits=partition_bits, force_wide=int(force_wide),
+                                       aggregation=aggregation)
         if ctas_per_sm:
             self.params.ctas_per_sm = ctas_per_sm
         col = make_column(keys, validity)
-        st = self._lib.sj_build(ctypes.byref(col), 1, ctypes.byref(self.params), None,
-                                _stream_handle(stream), ctypes.byref(self._handle))
-        L.check(st, "sj_build")
+        self.attached = [_as_pair(c) for c in attach]
+        if self.attached:
+            pay = [make_column(t, v) for t, v in self.attached]
+            st = self._lib.sj_build_ex(ctypes.byref(col), 1, _cols(pay), len(pay), ctypes.byref(self.params), None,
+                                       _stream_handle(stream), ctypes.byref(self._handle))
+            L.check(st, "sj_build_ex")
+        else:
+            st = self._lib.sj_build(ctypes.byref(col), 1, ctypes.byref(self.params), None,
+                                    _stream_handle(stream), ctypes.byref(self._handle))
+            L.check(st, "sj_build")
         self.build_rows = keys.numel()
 
     @property
@@ -160,7 +172,7 @@ class HashTable:
         return dc
 
     def probe_gather(self, probe_keys: torch.Tensor, probe_validity: Optional[torch.Tensor] = None,
-                     probe_payload=(), build_payload=(), *, capacity: Optional[int] = None,
+                     probe_payload=(), build_payload=(), *, attached: bool = False, capacity: Optional[int] = None,
                      out: Optional[JoinOutput] = None, d_count: Optional[torch.Tensor] = None,
                      stream: Optional[torch.cuda.Stream] = None, sync: bool = True) -> JoinOutput:
         """INNER probe fused with the payload gather.
@@ -177,16 +189,21 @@ class HashTable:
                 capacity = probe_keys.numel()
             else:
                 capacity = int(self.count(probe_keys, probe_validity, stream).item())
+        if attached:
+            if build_payload:
+                raise ValueError("attached=True gathers the attached build columns; pass no build_payload")
+            build_payload = self.attached
         if out is None:
             out = allocate_output(capacity, probe_payload, build_payload, dev)
         pin = [make_column(*_as_pair(c)) for c in probe_payload]
-        bin_ = [make_column(*_as_pair(c)) for c in build_payload]
+        bin_ = [] if attached else [make_column(*_as_pair(c)) for c in build_payload]
+        n_bin = len(build_payload)
         pout = [_mut(t, v) for t, v in zip(out.probe_payload, out.probe_payload_validity)]
         bout = [_mut(t, v) for t, v in zip(out.build_payload, out.build_payload_validity)]
         dc = d_count if d_count is not None else torch.empty(1, dtype=torch.int64, device=dev)
         key = make_column(probe_keys, probe_validity)
         st = self._lib.sj_probe_gather(
-            self.handle, ctypes.byref(key), 1, _cols(pin), len(pin), _cols(bin_), len(bin_),
+            self.handle, ctypes.byref(key), 1, _cols(pin), len(pin), None if attached else _cols(bin_), n_bin,
             out.probe_rid.data_ptr() if out.probe_rid is not None else None,
             out.build_rid.data_ptr() if out.build_rid is not None else None,
             _cols(pout, L.SjMutColumn), _cols(bout, L.SjMutColumn), capacity, None, _stream_handle(stream),

@@ -16,17 +16,21 @@ def dev_valid(words, dev):
     return None if words is None else torch.from_numpy(np.ascontiguousarray(words).view(np.int32)).to(dev)
 
 
-def gpu_join(inp, dev, **table_kw):
-    """Build + fused probe/gather on the GPU; returns (host arrays tuple, table info)."""
+def gpu_join(inp, dev, attach=False, **table_kw):
+    """Build + fused probe/gather on the GPU; returns (host arrays tuple, table info).
+    attach=True attaches the build payloads to the table (sj_build_ex) and gathers them from it."""
     from sirius_b200 import join as J
     bk, pk = dev_t(inp.build_keys, dev), dev_t(inp.probe_keys, dev)
     bv, pv = dev_valid(inp.build_validity, dev), dev_valid(inp.probe_validity, dev)
     bp = [dev_t(c, dev) for c in inp.build_payload]
     pp = [dev_t(c, dev) for c in inp.probe_payload]
-    with J.HashTable(bk, bv, **table_kw) as t:
+    with J.HashTable(bk, bv, attach=bp if attach else (), **table_kw) as t:
         info = t.info()
         cnt = int(t.count(pk, pv).item())
-        out = t.probe_gather(pk, pv, pp, bp).trimmed()
+        if attach:
+            out = t.probe_gather(pk, pv, pp, attached=True).trimmed()
+        else:
+            out = t.probe_gather(pk, pv, pp, bp).trimmed()
     torch.cuda.synchronize()
     assert cnt == out.count, (cnt, out.count)
     host = [out.probe_rid.cpu().numpy(), out.build_rid.cpu().numpy()]

@@ -244,3 +244,101 @@ def test_concurrent_probes_one_table(cuda):
             got = O.canonical(o.probe_rid[:n].cpu().numpy(), o.build_rid[:n].cpu().numpy())
             exp = O.canonical(r.probe_rid, r.build_rid)
             assert np.array_equal(got[0], exp[0]) and np.array_equal(got[1], exp[1])
+
+
+@pytest.mark.parametrize("n_probe", [1, 2, 3, 31, 33, 255, 257, 1023, 1025, 2047, 2049, 4097, 31784, 262145])
+def test_grouped_sizes_across_scan_blocks(cuda, n_probe):
+    """Output offsets of the grouped probe come from a multi-block scan; sweep entry counts around
+    its block and tile boundaries and check the exact row multiset."""
+    rng = np.random.default_rng(n_probe)
+    bk = rng.integers(0, 300, 2000).astype(np.int32)   # ~7 rows per key
+    pk = rng.integers(0, 330, n_probe).astype(np.int32)
+    inp = D.JoinInput("g", bk, pk, [rng.integers(0, 99, 2000).astype(np.int32)], [])
+    got, info = gpu_join(inp, cuda)
+    assert info.layout == 2
+    assert_same_rows(got, oracle_join(inp))
+
+
+@pytest.mark.parametrize("pbits", [1, 4, 7, 10])
+@pytest.mark.parametrize("attach", [False, True])
+def test_partitioned_distinct(cuda, pbits, attach):
+    """Radix-partitioned table (segments = partitions) and the partitioned probe path."""
+    inp = D.large(6, n_build=1 << 20, n_probe=3 << 20)
+    got, info = gpu_join(inp, cuda, attach=attach, partition_bits=pbits)
+    assert info.partition_bits == pbits and info.layout == 1
+    assert_same_rows(got, oracle_join(inp))
+
+
+def test_partitioned_auto_on_large_footprint(cuda):
+    inp = D.large(7, n_build=4 << 20, n_probe=1 << 20)
+    got, info = gpu_join(inp, cuda, attach=True)
+    assert info.partition_bits > 0   # 4M keys: slots + attached payloads exceed the L2 budget
+    assert_same_rows(got, oracle_join(inp))
+    got, info = gpu_join(inp, cuda, attach=True, partition_bits=-1)
+    assert info.partition_bits == 0
+    assert_same_rows(got, oracle_join(inp))
+
+
+@pytest.mark.parametrize("pbits", [-1, 3])
+def test_partitioned_with_nulls_and_payload_validity(cuda, pbits):
+    rng = np.random.default_rng(41)
+    nb, np_ = 200_000, 900_000
+    bk = rng.permutation(nb).astype(np.int64) * 3 - 100
+    pk = (rng.integers(0, nb + 5000, np_) * 3 - 100).astype(np.int64)
+    bpv, ppv = rng.random(nb) > 0.3, rng.random(np_) > 0.3
+    bp = rng.integers(0, 1 << 40, nb).astype(np.int64)
+    pp = rng.integers(0, 1 << 20, np_).astype(np.int32)
+    kbv, kpv = rng.random(nb) > 0.05, rng.random(np_) > 0.05
+    from sirius_b200 import join as J
+    for attach in (False, True):
+        bpay = [(dev_t(bp, cuda), dev_valid(O.pack_validity(bpv), cuda))]
+        ppay = [(dev_t(pp, cuda), dev_valid(O.pack_validity(ppv), cuda))]
+        with J.HashTable(dev_t(bk, cuda), dev_valid(O.pack_validity(kbv), cuda), partition_bits=pbits,
+                         attach=bpay if attach else ()) as t:
+            kw = dict(attached=True) if attach else dict(build_payload=bpay)
+            out = t.probe_gather(dev_t(pk, cuda), dev_valid(O.pack_validity(kpv), cuda), ppay, **kw).trimmed()
+        torch.cuda.synchronize()
+        ref = O.hash_join(bk, pk, O.pack_validity(kbv), O.pack_validity(kpv))
+        n = out.count
+        assert n == ref.rows
+        prid, brid = out.probe_rid.cpu().numpy(), out.build_rid.cpu().numpy()
+        a = O.canonical(prid, brid)
+        b = O.canonical(ref.probe_rid, ref.build_rid)
+        assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
+        assert np.array_equal(out.build_payload[0].cpu().numpy()[bpv[brid]], bp[brid][bpv[brid]])
+        assert np.array_equal(out.probe_payload[0].cpu().numpy()[ppv[prid]], pp[prid][ppv[prid]])
+        gv = O.unpack_validity(out.build_payload_validity[0].cpu().numpy().view(np.uint32), n)
+        pvv = O.unpack_validity(out.probe_payload_validity[0].cpu().numpy().view(np.uint32), n)
+        assert np.array_equal(gv, bpv[brid]) and np.array_equal(pvv, ppv[prid])
+
+
+@pytest.mark.parametrize("pbits", [2, 6])
+def test_partitioned_grouped(cuda, pbits):
+    """Duplicated build keys in a partitioned table: grouped ranges hold table positions."""
+    inp = D.skewed(8, n_build=1 << 19, n_probe=1 << 21, build_values=1 << 16, probe_values=1 << 17)
+    for attach in (False, True):
+        got, info = gpu_join(inp, cuda, attach=attach, partition_bits=pbits)
+        assert info.layout == 2 and info.partition_bits == pbits
+        assert_same_rows(got, oracle_join(inp))
+
+
+def test_attached_with_null_group(cuda):
+    """NULLs equal with NULL build keys: attached columns stay in row order."""
+    rng = np.random.default_rng(12)
+    bk = rng.integers(0, 50, 3000).astype(np.int32)
+    pk = rng.integers(0, 60, 9000).astype(np.int32)
+    inp = D.JoinInput("ng", bk, pk, [rng.integers(0, 1000, 3000).astype(np.int32)], [],
+                      O.pack_validity(rng.random(3000) > 0.1), O.pack_validity(rng.random(9000) > 0.1))
+    got, info = gpu_join(inp, cuda, attach=True, null_equality=1)
+    assert info.layout == 2
+    assert_same_rows(got, oracle_join(inp, nulls_equal=True))
+
+
+@pytest.mark.parametrize("agg", [1, 2])
+@pytest.mark.parametrize("pbits", [-1, 3])
+def test_output_aggregation_modes(cuda, agg, pbits):
+    """Per-warp and per-CTA output reservation give the same rows."""
+    inp = D.small(13, 300_000, 2_000_000)
+    for attach in (False, True):
+        got, info = gpu_join(inp, cuda, attach=attach, aggregation=agg, partition_bits=pbits)
+        assert_same_rows(got, oracle_join(inp))

@@ -127,19 +127,15 @@ __device__ __forceinline__ Record load_record(const void* p, int bytes) {
   }
   return r;
 }
-// Field of `width` bytes at byte offset `off` (aligned to its width) of a record. `off` is the
-// same for every lane (a launch parameter), so the switch is a uniform branch.
+// Field of `width` bytes at byte offset `off` (aligned to its width) of a record, picked with
+// predicated moves so the record stays in registers (no dynamic register indexing).
 __device__ __forceinline__ uint64_t record_field(const Record& r, int off, int width) {
+  const int wi = off >> 2;
   uint32_t lo = 0, hi = 0;
-  switch (off >> 2) {
-    case 0: lo = r.w[0]; hi = r.w[1]; break;
-    case 1: lo = r.w[1]; hi = r.w[2]; break;
-    case 2: lo = r.w[2]; hi = r.w[3]; break;
-    case 3: lo = r.w[3]; hi = r.w[4]; break;
-    case 4: lo = r.w[4]; hi = r.w[5]; break;
-    case 5: lo = r.w[5]; hi = r.w[6]; break;
-    case 6: lo = r.w[6]; hi = r.w[7]; break;
-    default: lo = r.w[7]; break;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    lo = (k == wi) ? r.w[k] : lo;
+    hi = (k == wi + 1) ? r.w[k] : hi;
   }
   if (width == 8) return ((uint64_t)hi << 32) | lo;
   if (width == 4) return lo;

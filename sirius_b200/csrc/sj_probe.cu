@@ -167,24 +167,15 @@ __device__ __forceinline__ void warp_write_out(const int32_t* s_row, int32_t* s_
                                                unsigned long long base_in, bool deferred, const GatherArgs& g) {
   const int lane = threadIdx.x & 31;
   if (g.rec) {
-    int32_t pr[KPT];
-#pragma unroll
-    for (int u = 0; u < KPT; ++u) {
-      const uint32_t i = lane + 32u * u;
-      pr[u] = 0;
-      if (i < tot) pr[u] = g.prid_map ? __ldg(g.prid_map + s_row[i]) : s_row[i];
+    const int64_t base = (int64_t)(deferred ? __shfl_sync(kFullMask, base_in, 0) : base_in);
+    if (g.out_prid) {
+      for (uint32_t i = lane; i < tot; i += 32) {
+        const int64_t p = base + i;
+        if (p < g.capacity) g.out_prid[p] = g.prid_map ? __ldg(g.prid_map + s_row[i]) : s_row[i];
+      }
     }
     Record r[KPT / 2];
     load_records(r, 0, s_rid, tot, g);
-    const int64_t base = (int64_t)(deferred ? __shfl_sync(kFullMask, base_in, 0) : base_in);
-    if (g.out_prid) {
-#pragma unroll
-      for (int u = 0; u < KPT; ++u) {
-        const uint32_t i = lane + 32u * u;
-        const int64_t p = base + i;
-        if (i < tot && p < g.capacity) g.out_prid[p] = pr[u];
-      }
-    }
     write_records(r, 0, tot, base, g);
     load_records(r, 1, s_rid, tot, g);
     write_records(r, 1, tot, base, g);
@@ -283,8 +274,6 @@ __global__ void __launch_bounds__(kProbeThreads, 4) probe_distinct_kernel(TableD
     const uint32_t incl = warp_inclusive_sum(cnt);
     const uint32_t tot = __shfl_sync(kFullMask, incl, 31);
     if (!CTA_AGG && tot == 0) continue;
-    unsigned long long early = 0;
-    if (!CTA_AGG && lane == 0) early = atomicAdd(g.d_count, (unsigned long long)tot);
     uint32_t sp = incl - cnt;
 #pragma unroll
     for (int j = 0; j < KPT; ++j) {
@@ -311,9 +300,8 @@ __global__ void __launch_bounds__(kProbeThreads, 4) probe_distinct_kernel(TableD
       __syncthreads();
       base = s_cta_base + s_wbase[warp];
     } else {
-      // lane 0's atomic result is only consumed by the stores, after the gather loads are issued
-      base = early;
-      deferred = true;
+      if (lane == 0) base = atomicAdd(g.d_count, (unsigned long long)tot);
+      deferred = true;  // broadcast from lane 0 inside the write-out
       __syncwarp();
     }
     if (tot) warp_write_out(s_row[warp], s_rid[warp], tot, base, deferred, g);

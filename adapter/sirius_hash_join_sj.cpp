@@ -1,0 +1,196 @@
+// Sirius-side glue for the sm_100a equi-join (see sirius_hash_join_sj.hpp).
+//
+// Call sites it replaces in src/op/sirius_physical_hash_join.cpp (INNER joins):
+//   build   :1614-1615 / :1852 cudf::distinct_hash_join(...)  -> sj_hash_table(..., unique=true)
+//           :1620          cudf::hash_join(...)              -> sj_hash_table(..., unique=false)
+//   probe   :1671 / :1688 / :1872 inner_join(...)            -> sj_hash_table::inner_join(...)
+//   gather  :1945-1954 gather_join_output(...)               -> (fused into inner_join above)
+#include "sirius_hash_join_sj.hpp"
+
+#include <cuda_runtime_api.h>
+
+#include <cstdint>
+#include <string>
+#include <utility>
+
+#include "cudf/null_mask.hpp"
+#include "rmm/device_buffer.hpp"
+
+namespace sirius::op::sj_adapter {
+
+namespace {
+
+// sj_alloc over an RMM resource: the join's device memory is the task's reservation.
+struct rmm_alloc_ctx {
+  rmm::device_async_resource_ref mr;
+};
+
+void* rmm_alloc(void* ctx, size_t bytes, sj_stream_t s) {
+  auto* c = static_cast<rmm_alloc_ctx*>(ctx);
+  try {
+    return c->mr.allocate_async(bytes, 256, rmm::cuda_stream_view(reinterpret_cast<cudaStream_t>(s)));
+  } catch (...) {
+    return nullptr;  // -> SJ_ERR_OOM -> rmm::out_of_memory in check()
+  }
+}
+
+void rmm_free(void* ctx, void* p, size_t bytes, sj_stream_t s) {
+  auto* c = static_cast<rmm_alloc_ctx*>(ctx);
+  c->mr.deallocate_async(p, bytes, 256, rmm::cuda_stream_view(reinterpret_cast<cudaStream_t>(s)));
+}
+
+int width_of(sj_type t) {
+  switch (t) {
+    case SJ_INT8:
+    case SJ_BOOL8: return 1;
+    case SJ_INT16: return 2;
+    case SJ_INT32:
+    case SJ_FLOAT32:
+    case SJ_UINT32: return 4;
+    default: return 8;
+  }
+}
+
+sj_stream_t raw(rmm::cuda_stream_view s) { return reinterpret_cast<sj_stream_t>(s.value()); }
+
+}  // namespace
+
+sj_type to_sj_type(cudf::data_type t) {
+  using cudf::type_id;
+  switch (t.id()) {
+    case type_id::INT8: return SJ_INT8;
+    case type_id::UINT8: return SJ_INT8;
+    case type_id::BOOL8: return SJ_BOOL8;
+    case type_id::INT16:
+    case type_id::UINT16: return SJ_INT16;
+    case type_id::INT32:
+    case type_id::TIMESTAMP_DAYS:
+    case type_id::DURATION_DAYS:
+    case type_id::DECIMAL32: return SJ_INT32;
+    case type_id::UINT32: return SJ_UINT32;
+    case type_id::INT64:
+    case type_id::TIMESTAMP_SECONDS:
+    case type_id::TIMESTAMP_MILLISECONDS:
+    case type_id::TIMESTAMP_MICROSECONDS:
+    case type_id::TIMESTAMP_NANOSECONDS:
+    case type_id::DURATION_SECONDS:
+    case type_id::DURATION_MILLISECONDS:
+    case type_id::DURATION_MICROSECONDS:
+    case type_id::DURATION_NANOSECONDS:
+    case type_id::DECIMAL64: return SJ_INT64;
+    case type_id::UINT64: return SJ_UINT64;
+    case type_id::FLOAT32: return SJ_FLOAT32;
+    case type_id::FLOAT64: return SJ_FLOAT64;
+    default: throw std::runtime_error("sj adapter: column type is not fixed-width");
+  }
+}
+
+sj_column to_sj(cudf::column_view const& c) {
+  sj_column s{};
+  const sj_type t = to_sj_type(c.type());
+  s.data            = static_cast<char const*>(c.head<void>()) + (int64_t)c.offset() * width_of(t);
+  s.validity        = c.nullable() ? c.null_mask() : nullptr;
+  s.validity_offset = c.offset();
+  s.num_rows        = c.size();
+  s.type            = t;
+  return s;
+}
+
+void check(sj_status st, char const* where) {
+  if (st == SJ_OK) return;
+  const std::string msg = std::string(where) + ": " + sj_status_string(st) + ": " + sj_last_error();
+  if (st == SJ_ERR_OOM) throw rmm::out_of_memory(msg.c_str());
+  throw std::runtime_error(msg);
+}
+
+sj_hash_table::sj_hash_table(cudf::table_view const& build_keys, cudf::table_view const& build_payload,
+                             cudf::null_equality nulls, bool unique_build_keys, rmm::cuda_stream_view stream,
+                             rmm::device_async_resource_ref mr)
+  : mr_(mr), stream_(stream)
+{
+  if (build_keys.num_columns() != 1) throw std::runtime_error("sj adapter: one equi-key column");
+  const sj_column key = to_sj(build_keys.column(0));
+  std::vector<sj_column> pay;
+  for (cudf::size_type c = 0; c < build_payload.num_columns(); ++c) {
+    pay.push_back(to_sj(build_payload.column(c)));
+    build_types_.push_back(build_payload.column(c).type());
+    build_nullable_.push_back(build_payload.column(c).nullable());
+  }
+  sj_join_params p;
+  sj_default_params(&p);
+  p.layout        = unique_build_keys ? SJ_LAYOUT_DISTINCT : SJ_LAYOUT_AUTO;
+  p.null_equality = nulls == cudf::null_equality::EQUAL ? SJ_NULLS_EQUAL : SJ_NULLS_UNEQUAL;
+  rmm_alloc_ctx ctx{mr};
+  const sj_alloc a{&ctx, rmm_alloc, rmm_free};
+  // sj_build_ex synchronizes the stream, as the operator does after building (:1622)
+  check(sj_build_ex(&key, 1, pay.data(), (int32_t)pay.size(), &p, &a, raw(stream), &table_), "sj_build_ex");
+}
+
+sj_hash_table::~sj_hash_table() { sj_table_destroy(table_, raw(stream_)); }
+
+std::unique_ptr<cudf::table> sj_hash_table::inner_join(cudf::table_view const& probe_keys,
+                                                       cudf::table_view const& probe_payload,
+                                                       rmm::cuda_stream_view stream,
+                                                       rmm::device_async_resource_ref mr) const
+{
+  if (probe_keys.num_columns() != 1) throw std::runtime_error("sj adapter: one equi-key column");
+  const sj_column key = to_sj(probe_keys.column(0));
+  rmm_alloc_ctx ctx{mr};
+  const sj_alloc a{&ctx, rmm_alloc, rmm_free};
+
+  // output size: a DISTINCT table never returns more rows than it is probed with; otherwise count
+  sj_table_info info{};
+  check(sj_table_get_info(table_, &info), "sj_table_get_info");
+  rmm::device_buffer d_count(sizeof(int64_t), stream, mr);
+  int64_t capacity = key.num_rows;
+  if (info.layout != SJ_LAYOUT_DISTINCT) {
+    check(sj_probe_count(table_, &key, 1, &a, raw(stream), static_cast<int64_t*>(d_count.data())), "sj_probe_count");
+    cudaMemcpyAsync(&capacity, d_count.data(), sizeof(int64_t), cudaMemcpyDeviceToHost, stream.value());
+    cudaStreamSynchronize(stream.value());
+  }
+
+  // outputs: [probe payload columns..., build payload columns...] plus their null masks
+  std::vector<sj_column> pin;
+  std::vector<rmm::device_buffer> data, masks;
+  std::vector<cudf::data_type> types;
+  std::vector<sj_mut_column> pout, bout;
+  const size_t mask_bytes = (size_t)((capacity + 31) / 32) * sizeof(uint32_t);
+  auto add_out = [&](cudf::data_type t, bool nullable, std::vector<sj_mut_column>& outs) {
+    const sj_type st = to_sj_type(t);
+    data.emplace_back((size_t)capacity * width_of(st), stream, mr);
+    masks.emplace_back(nullable ? mask_bytes : 0, stream, mr);
+    types.push_back(t);
+    sj_mut_column m{};
+    m.data     = data.back().data();
+    m.validity = nullable ? static_cast<uint32_t*>(masks.back().data()) : nullptr;
+    m.type     = st;
+    outs.push_back(m);
+  };
+  for (cudf::size_type c = 0; c < probe_payload.num_columns(); ++c) {
+    pin.push_back(to_sj(probe_payload.column(c)));
+    add_out(probe_payload.column(c).type(), probe_payload.column(c).nullable(), pout);
+  }
+  for (size_t c = 0; c < build_types_.size(); ++c) add_out(build_types_[c], build_nullable_[c], bout);
+
+  check(sj_probe_gather(table_, &key, 1, pin.data(), (int32_t)pin.size(), /*attached build payloads*/ nullptr,
+                        (int32_t)bout.size(), nullptr, nullptr, pout.data(), bout.data(), capacity, &a, raw(stream),
+                        static_cast<int64_t*>(d_count.data())),
+        "sj_probe_gather");
+  int64_t rows = 0;
+  cudaMemcpyAsync(&rows, d_count.data(), sizeof(int64_t), cudaMemcpyDeviceToHost, stream.value());
+  cudaStreamSynchronize(stream.value());
+  if (rows > capacity) throw std::runtime_error("sj adapter: probe produced more rows than counted");
+
+  std::vector<std::unique_ptr<cudf::column>> cols;
+  for (size_t c = 0; c < data.size(); ++c) {
+    const bool nullable      = masks[c].size() > 0;
+    const auto n             = static_cast<cudf::size_type>(rows);
+    const cudf::size_type nc = nullable ? cudf::null_count(static_cast<cudf::bitmask_type const*>(masks[c].data()),
+                                                           0, n, stream)
+                                        : 0;
+    cols.push_back(std::make_unique<cudf::column>(types[c], n, std::move(data[c]), std::move(masks[c]), nc));
+  }
+  return std::make_unique<cudf::table>(std::move(cols), stream);
+}
+
+}  // namespace sirius::op::sj_adapter

@@ -1,0 +1,59 @@
+// Sirius-side glue for the sm_100a equi-join: what `sirius_physical_hash_join::execute`
+// (src/op/sirius_physical_hash_join.cpp:1527-1955) calls instead of cuDF for INNER joins.
+//
+// It maps cudf::column_view to sj_column, wraps the task's RMM resource as an sj_alloc (so the
+// join's device memory is charged to the task's cuCascade reservation,
+// src/pipeline/gpu_pipeline_task.cpp:523-525), and turns sj_status into the exceptions the
+// operator's callers already handle: SJ_ERR_OOM -> rmm::out_of_memory (the OOM reschedule path,
+// src/pipeline/gpu_pipeline_task.cpp:386-437), anything else -> std::runtime_error.
+#pragma once
+
+#include <memory>
+#include <stdexcept>
+#include <vector>
+
+#include "cudf/column/column.hpp"
+#include "cudf/table/table.hpp"
+#include "cudf/table/table_view.hpp"
+#include "rmm/cuda_stream_view.hpp"
+#include "rmm/resource_ref.hpp"
+#include "sj/sj_join.h"
+
+namespace sirius::op::sj_adapter {
+
+/// sj_type of a fixed-width cuDF type (DATE / TIMESTAMP / DURATION are stored as INT32 / INT64).
+sj_type to_sj_type(cudf::data_type t);
+
+/// Read-only view of a column: data at row 0, the null mask with the view's bit offset.
+sj_column to_sj(cudf::column_view const& c);
+
+/// Throws rmm::out_of_memory for SJ_ERR_OOM, std::runtime_error otherwise (no-op for SJ_OK).
+void check(sj_status st, char const* where);
+
+/// The built table of one BUILD_PROBE partition slot: replaces cudf::hash_join /
+/// cudf::distinct_hash_join in per_partition_build_state
+/// (src/include/op/sirius_physical_hash_join.hpp:409-421). It keeps a copy of the projected build
+/// columns (rhs_output_columns) so a probe's gather never touches the build batch at random.
+class sj_hash_table {
+ public:
+  sj_hash_table(cudf::table_view const& build_keys, cudf::table_view const& build_payload,
+                cudf::null_equality nulls, bool unique_build_keys, rmm::cuda_stream_view stream,
+                rmm::device_async_resource_ref mr);
+  ~sj_hash_table();
+  sj_hash_table(sj_hash_table const&)            = delete;
+  sj_hash_table& operator=(sj_hash_table const&) = delete;
+
+  /// INNER probe + gather_join_output in one call: returns the output table
+  /// [probe_payload columns..., build payload columns...] (src/op/sirius_physical_hash_join.cpp:1350-1355).
+  std::unique_ptr<cudf::table> inner_join(cudf::table_view const& probe_keys, cudf::table_view const& probe_payload,
+                                          rmm::cuda_stream_view stream, rmm::device_async_resource_ref mr) const;
+
+ private:
+  sj_table* table_ = nullptr;
+  std::vector<cudf::data_type> build_types_;
+  std::vector<bool> build_nullable_;
+  rmm::device_async_resource_ref mr_;
+  rmm::cuda_stream_view stream_;
+};
+
+}  // namespace sirius::op::sj_adapter

@@ -1,9 +1,6 @@
 // Stand-in: the subset of rmm::cuda_stream_view the adapter uses.
 #pragma once
-struct CUstream_st;
-#ifndef __CUDA_RUNTIME_H__
-typedef struct CUstream_st* cudaStream_t;
-#endif
+#include "cuda_runtime_api.h"
 namespace rmm {
 class cuda_stream_view {
  public:

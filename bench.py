@@ -226,16 +226,16 @@ def run_sj(args):
 
     from sirius_b200 import datagen as D
     from sirius_b200 import join as J
+    from sirius_b200 import multigpu as MG
     from sirius_b200 import _lib
 
     _lib.load()
     # every rank: the same build side; its own probe shard (seed stream offset by rank)
     inp = D.large(args.seed, args.n_build, args.n_probe)
     if rank > 0:
-        # same build side; this rank's probe shard drawn from it with the rank's own stream
-        rng = np.random.default_rng([args.seed, rank])
-        inp.probe_keys = inp.build_keys[rng.integers(0, args.n_build, args.n_probe)]
-        inp.probe_payload = [rng.integers(-2**63, 2**63 - 1, args.n_probe, dtype=np.int64, endpoint=True)]
+        # same (replicated) build side; this rank's own probe shard
+        keys, pay = MG.probe_shard(inp.build_keys, args.n_probe, args.seed, rank)
+        inp.probe_keys, inp.probe_payload = keys, [pay]
     bk = torch.from_numpy(inp.build_keys).to(dev)
     pk = torch.from_numpy(inp.probe_keys).to(dev)
     bp = [torch.from_numpy(c).to(dev) for c in inp.build_payload]
@@ -299,12 +299,8 @@ def run_sj(args):
         dist.barrier()
     total_ms = t_all0.elapsed_time(t_all1)
     per_launch = [s.elapsed_time(e) for s, e in zip(starts, ends)]
-    t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    max_ms = float(t.item())
-    rows_all = args.n_probe * args.steps * world
-    value = rows_all / (max_ms / 1e3) / 1e6
+    max_ms = MG.max_over_ranks(total_ms, dev)
+    value = MG.weak_scaling_value(args.n_probe, args.steps, world, max_ms)
     clocks = clk.summary()
 
     # ---- e2e: one-shot join through the C ABI from pinned host buffers ----
@@ -348,10 +344,7 @@ def run_sj(args):
         torch.cuda.synchronize()
         e_ms = e0.elapsed_time(e1)
         wall_ms = (time.perf_counter() - w0) * 1e3
-        te = torch.tensor([max(e_ms, wall_ms)], dtype=torch.float64, device=dev)
-        if world > 1:
-            dist.all_reduce(te, op=dist.ReduceOp.MAX)
-        e_max = float(te.item())
+        e_max = MG.max_over_ranks(max(e_ms, wall_ms), dev)
         assert int(d_count.item()) == args.n_probe
         e2e = {"value": round(args.n_probe * args.e2e_steps * world / (e_max / 1e3) / 1e6, 3),
                "unit": "Mtuples/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),

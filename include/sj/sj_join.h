@@ -239,6 +239,32 @@ SJ_EXPORT sj_status sj_inner_join(const sj_column* build_keys, const sj_column* 
                                   const sj_join_params* params, const sj_alloc* alloc,
                                   sj_stream_t stream, int64_t* d_count);
 
+/* The one-shot INNER join of sj_inner_join for callers that cannot allocate device memory: code
+ * held to a device-memory reservation that is already fully committed (an allocation attempt
+ * there would be refused and rescheduled as out-of-memory), latency-critical host threads that
+ * must not wait in the driver's allocator, and hosts whose allocator belongs to another component.
+ * No counterpart in the reference: Sirius's join always allocates through its memory pool.
+ * Every byte of scratch (hash table, build statistics, grouped-probe match list) comes from one
+ * 64 MiB `static __device__` array per GPU, held by every GPU that loads this library until the
+ * process exits; no cudaMalloc, cudaFree or allocator callback is used. Outputs follow
+ * sj_probe_gather's contract (caller-provided device buffers, *d_count = matches). Inputs whose
+ * worst-case scratch exceeds the arena are rejected with SJ_ERR_INVALID before any GPU work (about
+ * 1M build rows with a few million probe rows fit). The table is never radix-partitioned.
+ * All calls share the array and leave their data in it; each call re-initialises what it reads,
+ * but calls that overlap on the GPU race: serialise them (one stream, or synchronise between).
+ * The first call on a device looks up the array's device address (cudaGetSymbolAddress) with that
+ * device current; make it before any stream capture begins on the device. Synchronizes `stream`
+ * like sj_build. */
+SJ_EXPORT sj_status sj_inner_join_noalloc(const sj_column* build_keys, const sj_column* probe_keys,
+                                          int32_t num_keys, const sj_column* probe_payload,
+                                          int32_t num_probe_payload, const sj_column* build_payload,
+                                          int32_t num_build_payload, int32_t* out_probe_rid,
+                                          int32_t* out_build_rid,
+                                          const sj_mut_column* out_probe_payload,
+                                          const sj_mut_column* out_build_payload, int64_t capacity,
+                                          const sj_join_params* params, sj_stream_t stream,
+                                          int64_t* d_count);
+
 /* ---------------------------------------------------------------------------------------------
  * Diagnostics.
  * ------------------------------------------------------------------------------------------- */

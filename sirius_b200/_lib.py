@@ -76,6 +76,9 @@ SIGNATURES = {
     "sj_inner_join": (c_int32, [_P(SjColumn), _P(SjColumn), c_int32, _P(SjColumn), c_int32, _P(SjColumn), c_int32,
                                 c_void_p, c_void_p, _P(SjMutColumn), _P(SjMutColumn), c_int64, _P(SjJoinParams),
                                 _P(SjAlloc), c_void_p, c_void_p]),
+    "sj_inner_join_noalloc": (c_int32, [_P(SjColumn), _P(SjColumn), c_int32, _P(SjColumn), c_int32, _P(SjColumn),
+                                        c_int32, c_void_p, c_void_p, _P(SjMutColumn), _P(SjMutColumn), c_int64,
+                                        _P(SjJoinParams), c_void_p, c_void_p]),
     "sj_status_string": (c_char_p, [c_int32]),
     "sj_last_error": (c_char_p, []),
     "sj_version": (c_int32, []),

@@ -1,0 +1,151 @@
+// sj_inner_join_noalloc: the one-shot INNER join for callers that cannot allocate device memory.
+//
+// Who needs it: code that runs under a device-memory budget it must not exceed or grow (for
+// example a task whose reservation from Sirius's memory manager is already fully committed, where
+// any allocation attempt would be refused and turned into an out-of-memory reschedule), code on a
+// latency-critical host thread that must not wait in the driver's allocator (cudaMalloc can
+// synchronize the whole device), and hosts whose device allocator belongs to another component
+// and may not be called from this library. For them this entry point takes every byte of scratch
+// (the hash table, its build statistics, the grouped-probe match list) from one statically
+// allocated device array instead of cudaMalloc / cudaMallocAsync / an allocator callback.
+//
+// Limits and rules:
+//   - The arena is kNoAllocArenaBytes = 64 MiB per GPU, declared below as a file-scope
+//     `static __device__` array: every GPU on which this library is loaded holds it until the
+//     process exits, whether or not the entry point is ever called.
+//   - A call whose worst-case need exceeds the arena is rejected with SJ_ERR_INVALID before any
+//     GPU work (about 1M build rows and a few million probe rows fit; the exact need is printed).
+//   - Radix partitioning and attached payloads are not used (the table is built unpartitioned).
+//   - All calls share the arena and leave their data in it; each call re-initialises everything it
+//     reads (slots, counters, offsets) before use, so stale contents never leak into a result.
+//     Calls that overlap on the GPU race on the arena: issue them on one stream, or synchronise.
+//   - The arena's device address is looked up with cudaGetSymbolAddress the first time the entry
+//     point runs on a device (with that device current); make that first call before any stream
+//     capture begins on the device.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "sj_internal.h"
+
+namespace sj {
+
+constexpr size_t kNoAllocArenaBytes = 64ull << 20;
+
+// The arena. In host code `g_noalloc_arena` only names the symbol; its device address comes from
+// cudaGetSymbolAddress below.
+static __device__ __align__(256) unsigned char g_noalloc_arena[kNoAllocArenaBytes];
+
+static std::mutex g_noalloc_mu;
+static std::vector<void*> g_noalloc_base;  // per device: the arena's device address
+
+static sj_status noalloc_arena(void** out) {
+  int dev = 0;
+  SJ_CUDA_TRY(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  if ((int)g_noalloc_base.size() <= dev) g_noalloc_base.resize(dev + 1, nullptr);
+  if (!g_noalloc_base[dev]) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_arena);
+    if (e != cudaSuccess || p == nullptr)
+      return set_error(SJ_ERR_DEVICE, std::string("cudaGetSymbolAddress of the static arena failed: ") +
+                                          cudaGetErrorString(e));
+    g_noalloc_base[dev] = p;
+  }
+  *out = g_noalloc_base[dev];
+  return SJ_OK;
+}
+
+// Bump allocator over the arena for one call: frees are no-ops, the next call starts over.
+struct Bump {
+  char* base;
+  size_t cap;
+  size_t used;
+};
+
+static void* bump_alloc(void* ctx, size_t bytes, sj_stream_t) {
+  Bump* b = static_cast<Bump*>(ctx);
+  const size_t off = (b->used + 255) & ~(size_t)255;
+  if (off > b->cap || bytes > b->cap - off) return nullptr;
+  b->used = off + bytes;
+  return b->base + off;
+}
+
+static void bump_free(void*, void*, size_t, sj_stream_t) {}
+
+static size_t a256(size_t b) { return (std::max<size_t>(b, 16) + 255) & ~(size_t)255; }
+
+// Worst case over slot encodings and layouts of what build + probe take from the allocator.
+static size_t noalloc_need(int64_t n_build, int64_t n_probe, double lf) {
+  const double keys = (double)std::max<int64_t>(n_build, 1) / lf;
+  size_t buckets = 1;
+  while ((double)buckets * 2.0 < keys) buckets <<= 1;  // wide slots: 2 per bucket (more buckets)
+  const size_t slot_bytes = buckets * 32;
+  const size_t nslots = buckets * 4;
+  size_t need = a256(64);                         // build statistics
+  need += 2 * a256(slot_bytes);                   // slots + the shrunken copy of a grouped build
+  need += a256((nslots + 1) * 4) + a256((nslots + 2) * 4);  // group counts + offsets
+  need += a256((size_t)std::max<int64_t>(n_build, 1) * 4);  // grouped row positions
+  need += a256(8192);                             // scan block sums
+  const size_t np = (size_t)std::max<int64_t>(n_probe, 1);
+  need += a256(3 * a256(np * 4) + a256((np + 1) * 8) + 8192 + 256);  // grouped probe match list
+  return need;
+}
+
+}  // namespace sj
+
+using namespace sj;
+
+extern "C" SJ_EXPORT sj_status sj_inner_join_noalloc(
+    const sj_column* build_keys, const sj_column* probe_keys, int32_t num_keys, const sj_column* probe_payload,
+    int32_t num_probe_payload, const sj_column* build_payload, int32_t num_build_payload, int32_t* out_probe_rid,
+    int32_t* out_build_rid, const sj_mut_column* out_probe_payload, const sj_mut_column* out_build_payload,
+    int64_t capacity, const sj_join_params* params, sj_stream_t stream, int64_t* d_count) {
+  clear_error();
+  if (num_keys != 1) return set_error(SJ_ERR_INVALID, "exactly one key column is supported");
+  if (!build_keys || !probe_keys || !d_count)
+    return set_error(SJ_ERR_INVALID, "build_keys, probe_keys and d_count are required");
+  sj_join_params p;
+  sj_default_params(&p);
+  if (params) {
+    p.layout = params->layout;
+    p.null_equality = params->null_equality;
+    if (params->load_factor > 0.0f) p.load_factor = params->load_factor;
+    p.force_wide = params->force_wide;
+    if (params->ctas_per_sm > 0) p.ctas_per_sm = params->ctas_per_sm;
+    p.aggregation = params->aggregation;
+  }
+  p.partition_bits = -1;  // unpartitioned: no row store, no partition buffers
+  if (!(p.load_factor > 0.0f && p.load_factor < 1.0f)) return set_error(SJ_ERR_INVALID, "load_factor must be in (0, 1)");
+  const size_t need = noalloc_need(build_keys->num_rows, probe_keys->num_rows, p.load_factor);
+  if (need > kNoAllocArenaBytes)
+    return set_error(SJ_ERR_INVALID, "sj_inner_join_noalloc: " + std::to_string(build_keys->num_rows) +
+                                         " build rows and " + std::to_string(probe_keys->num_rows) +
+                                         " probe rows need up to " + std::to_string(need) +
+                                         " bytes of scratch; the static arena holds " +
+                                         std::to_string(kNoAllocArenaBytes) + " bytes");
+  void* base = nullptr;
+  SJ_TRY(noalloc_arena(&base));
+  Bump bump{static_cast<char*>(base), kNoAllocArenaBytes, 0};
+  const sj_alloc a{&bump, bump_alloc, bump_free};
+  const Allocator alloc(&a);
+  const cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  sj_table* t = nullptr;
+  try {
+    SJ_TRY(build_table(build_keys[0], nullptr, 0, p, alloc, s, &t));
+    const GatherSpec g{probe_payload, num_probe_payload, build_payload, num_build_payload, out_probe_rid,
+                       out_build_rid, out_probe_payload, out_build_payload, capacity};
+    const sj_status st = probe_gather(t, probe_keys[0], g, alloc, s, d_count);
+    const std::string msg = sj_last_error();
+    destroy_table(t, s);
+    if (st != SJ_OK) return set_error(st, msg);
+    return SJ_OK;
+  } catch (const std::exception& e) {
+    if (t) destroy_table(t, s);
+    return set_error(SJ_ERR_DEVICE, e.what());
+  }
+}

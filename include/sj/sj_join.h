@@ -239,6 +239,66 @@ SJ_EXPORT sj_status sj_inner_join(const sj_column* build_keys, const sj_column* 
                                   const sj_join_params* params, const sj_alloc* alloc,
                                   sj_stream_t stream, int64_t* d_count);
 
+/* ---------------------------------------------------------------------------------------------
+ * Batched joins: thousands of independent small INNER joins in one persistent launch.
+ * ------------------------------------------------------------------------------------------- */
+
+/* One join of a batch. Keys are SJ_INT32 or SJ_INT64 (one type for the whole batch); each side
+ * carries at most one payload column (data == NULL: none). Outputs follow sj_probe_gather:
+ * every match writes probe row id, build row id and the payloads at one position < capacity;
+ * the join's match count is read with sj_batch_plan_counts. Duplicated build keys are allowed
+ * (all matches are produced). Key validity is honoured (NULL never matches). */
+typedef struct sj_batch_join {
+  sj_column build_key;
+  sj_column build_payload;
+  sj_column probe_key;
+  sj_column probe_payload;
+  int32_t* out_probe_rid;
+  int32_t* out_build_rid;
+  sj_mut_column out_probe_payload;
+  sj_mut_column out_build_payload;
+  int64_t capacity;
+} sj_batch_join;
+
+/* Tunables of the batched launch (0 = default; the autotuner picks them per GPU and size class). */
+typedef struct sj_batch_params {
+  int32_t block_size;   /* threads per CTA: 128, 256 or 512; default 256 */
+  int32_t group_width;  /* lanes cooperating on one probe key: 1, 2, 4 or 8; default 1 */
+  float load_factor;    /* table slots in use / slots; default 0.5 */
+  int32_t tile_rows;    /* rows per work item; default 4096 */
+  int32_t ctas_per_sm;  /* resident CTAs per SM of the persistent grid; default 4 */
+  int32_t reserved[7];
+} sj_batch_params;
+
+typedef struct sj_batch_plan sj_batch_plan;
+
+/* Plan a batch: sizes every join's table, lays out one table arena and the work queue (every
+ * join's build tiles, then every join's probe tiles), and uploads the descriptors. The column
+ * pointers are read by each launch, so the caller may refill the same buffers between launches.
+ * Allocates through `alloc`; stream-ordered. */
+SJ_EXPORT sj_status sj_batch_plan_create(const sj_batch_join* joins, int32_t num_joins,
+                                         const sj_batch_params* params, const sj_alloc* alloc,
+                                         sj_stream_t stream, sj_batch_plan** out);
+
+/* Run every join of the plan in ONE persistent kernel launch (plus memset nodes that reset the
+ * tables, counters and queue). A probe work item waits — bounded, then flags an error — until its
+ * join's build tiles are done. Stream-ordered, no host synchronisation, capturable. */
+SJ_EXPORT sj_status sj_batch_plan_launch(sj_batch_plan* plan, sj_stream_t stream);
+
+/* Capture sj_batch_plan_launch into a CUDA graph once (on `stream`) and replay it: the whole batch
+ * is one graph launch. */
+SJ_EXPORT sj_status sj_batch_plan_replay(sj_batch_plan* plan, sj_stream_t stream);
+
+/* The comparison point: the same joins with one build launch and one probe launch per join. */
+SJ_EXPORT sj_status sj_batch_plan_launch_per_join(sj_batch_plan* plan, sj_stream_t stream);
+
+/* Copy the per-join match counts (int64[num_joins], device) and the plan's error word (device
+ * int32: 0 = ok, 1 = a probe item timed out waiting for its build) into caller memory. */
+SJ_EXPORT sj_status sj_batch_plan_counts(const sj_batch_plan* plan, int64_t* d_counts, int32_t* d_error,
+                                         sj_stream_t stream);
+
+SJ_EXPORT sj_status sj_batch_plan_destroy(sj_batch_plan* plan, sj_stream_t stream);
+
 /* The one-shot INNER join of sj_inner_join for callers that cannot allocate device memory: code
  * held to a device-memory reservation that is already fully committed (an allocation attempt
  * there would be refused and rescheduled as out-of-memory), latency-critical host threads that

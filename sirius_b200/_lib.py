@@ -56,6 +56,17 @@ class SjTableInfo(Structure):
                 ("max_group", c_int32)]
 
 
+class SjBatchJoin(Structure):
+    _fields_ = [("build_key", SjColumn), ("build_payload", SjColumn), ("probe_key", SjColumn),
+                ("probe_payload", SjColumn), ("out_probe_rid", c_void_p), ("out_build_rid", c_void_p),
+                ("out_probe_payload", SjMutColumn), ("out_build_payload", SjMutColumn), ("capacity", c_int64)]
+
+
+class SjBatchParams(Structure):
+    _fields_ = [("block_size", c_int32), ("group_width", c_int32), ("load_factor", c_float),
+                ("tile_rows", c_int32), ("ctas_per_sm", c_int32), ("reserved", c_int32 * 7)]
+
+
 class SjKernelTime(Structure):
     _fields_ = [("name", c_char_p), ("ms", c_float), ("reserved", c_int32)]
 
@@ -83,6 +94,13 @@ SIGNATURES = {
     "sj_last_error": (c_char_p, []),
     "sj_version": (c_int32, []),
     "sj_timing_enable": (None, [c_int32]),
+    "sj_batch_plan_create": (c_int32, [_P(SjBatchJoin), c_int32, _P(SjBatchParams), _P(SjAlloc), c_void_p,
+                                       _P(c_void_p)]),
+    "sj_batch_plan_launch": (c_int32, [c_void_p, c_void_p]),
+    "sj_batch_plan_replay": (c_int32, [c_void_p, c_void_p]),
+    "sj_batch_plan_launch_per_join": (c_int32, [c_void_p, c_void_p]),
+    "sj_batch_plan_counts": (c_int32, [c_void_p, c_void_p, c_void_p, c_void_p]),
+    "sj_batch_plan_destroy": (c_int32, [c_void_p, c_void_p]),
     "sj_timing_collect": (c_int32, [_P(SjKernelTime), c_int32]),
 }
 

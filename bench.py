@@ -56,7 +56,11 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--partition-bits", type=int, default=0)
     ap.add_argument("--aggregation", type=int, default=0)
-    ap.add_argument("--workload", default="large", choices=["large", "batched"])
+    ap.add_argument("--workload", default="large", choices=["large", "batched", "served"])
+    ap.add_argument("--autotune", action="store_true", help="batched: choose launch parameters by the autotuner")
+    ap.add_argument("--requests", type=int, default=2000)
+    ap.add_argument("--slots", type=int, default=4)
+    ap.add_argument("--served-max-rows", type=int, default=20_000_000)
     ap.add_argument("--joins", type=int, default=4096)
     ap.add_argument("--wave-probe-rows", type=int, default=1_500_000_000)
     ap.add_argument("--block-size", type=int, default=0)
@@ -456,6 +460,16 @@ def run_batched(args):
     sizes = D.batched_sizes(args.seed, args.joins)
     params = B.batch_params(block_size=args.block_size, group_width=args.group_width, tile_rows=args.tile_rows,
                             load_factor=args.load_factor)
+    tuned = None
+    if args.autotune:
+        from sirius_b200 import autotune as A
+        # 256 joins spread over the size distribution
+        sample = np.sort(sizes)[np.linspace(0, len(sizes) - 1, 256).astype(int)]
+        t0 = time.perf_counter()
+        tuned = A.tune_batch(batched_wave_specs(sample, 0, dev, args.seed + 1), key_type="int32")
+        tuned = dict(tuned, tune_seconds=round(time.perf_counter() - t0, 2))
+        params = B.batch_params(**{k: v for k, v in tuned.items() if k in A.BATCH_SPACE})
+        torch.cuda.empty_cache()
     # waves bounded by probe rows so inputs + outputs + tables fit in HBM
     waves, cur, acc = [], [], 0
     for i, nb in enumerate(sizes):
@@ -515,11 +529,144 @@ def run_batched(args):
                                f"probe 10x build uniform over 1.2x the key range, int32 payloads",
                    "joins": args.joins, "waves": len(waves), "build_rows": build_rows, "probe_rows": probe_rows,
                    "matches": matches, "params": {"block_size": params.block_size, "group_width": params.group_width,
-                                                  "tile_rows": params.tile_rows, "load_factor": params.load_factor}},
+                                                  "tile_rows": params.tile_rows,
+                                                  "load_factor": round(params.load_factor, 3)},
+                   "autotuned": tuned},
         "persistent_launch_ms": round(t_launch, 3), "graph_replay_ms": round(t_graph, 3),
         "one_launch_per_join_ms": round(t_per_join, 3),
         "speedup_vs_per_join": round(t_per_join / t_graph, 3),
         "gpu_launches": len(waves), "clocks": clk.summary(),
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# --------------------------------------------------------------------------------------------
+# served workload: resident tables, a stream of probe requests
+# --------------------------------------------------------------------------------------------
+def _pct(xs, q):
+    xs = sorted(xs)
+    return xs[min(len(xs) - 1, int(round(q / 100 * (len(xs) - 1))))]
+
+
+def run_served(args):
+    """8 resident tables (unique int64 keys, 1M..48M rows, one int64 payload); requests pick a table
+    uniformly and probe a log-uniform 10K..20M keys at a 70% hit rate. Each request is served by
+    the join server (admission against a 120 GiB budget, `--slots` concurrent streams) and, for
+    comparison, by the same server with one slot (serial one-at-a-time execution). Both see the
+    same requests: all at once (saturation: throughput) and as Poisson arrivals at 0.5, 0.8 and
+    0.95 x the serial capacity (latency p50/p99, submit to the request's last GPU operation)."""
+    import torch
+    from sirius_b200 import datagen as D
+    from sirius_b200 import serve as S
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    rows = D.SERVED_TABLE_ROWS
+    tables = [D.served_table_device(args.seed, t, n, dev) for t, n in enumerate(rows)]
+    hi = args.served_max_rows
+    pools = [D.served_probe_pool(args.seed, t, k, hi) for t, (k, _) in enumerate(tables)]
+    ts, sizes, starts = D.served_requests(args.seed, args.requests, len(rows), 1e4, hi)
+    reqs = []
+    for i in range(args.requests):
+        t, m = int(ts[i]), int(sizes[i])
+        off = int(starts[i] * (hi - m)) & ~1  # 16-byte aligned windows
+        reqs.append((t, pools[t][off:off + m]))
+    probe_rows = int(sizes.sum())
+    torch.cuda.synchronize()
+
+    def make(slots):
+        srv = S.JoinServer(slots=slots, memory_budget_bytes=120 << 30)
+        tids = [srv.add_table(k, attach=[p]) for k, p in tables]
+        return srv, tids
+
+    def run(srv, tids, arrivals, base_id):
+        """Submit every request at t0 + arrivals[i]; returns {i: (latency s, count)}, makespan s."""
+        n = len(reqs)
+        err = []
+
+        def submitter():
+            t0 = time.perf_counter()
+            try:
+                for i, (t, pk) in enumerate(reqs):
+                    if arrivals is not None:
+                        d = t0 + arrivals[i] - time.perf_counter()
+                        if d > 0:
+                            time.sleep(d)
+                    srv.submit(tids[t], pk, base_id + i, sync=False)
+            except Exception as e:  # surfaced below
+                err.append(e)
+
+        th = threading.Thread(target=submitter)
+        th.start()
+        got = {}
+        while len(got) < n:
+            if err and not th.is_alive() and not srv._inflight:
+                break
+            for r in srv.poll(256, wait_ms=20):
+                assert r.status == 0, f"request {r.request_id} failed with status {r.status}"
+                got[r.request_id - base_id] = (r.t_done - r.t_submit, r.count, r.t_submit, r.t_done)
+                srv.release(r.request_id)
+        th.join()
+        if err:
+            raise err[0]
+        makespan = max(v[3] for v in got.values()) - min(v[2] for v in got.values())
+        return got, makespan
+
+    def warm(srv, tids):
+        for t in range(len(rows)):
+            for m in (10_000, 1_000_000):
+                srv.submit(tids[t], pools[t][:m], 10**9 + t * 10 + (m > 10_000), sync=False)
+        left = 2 * len(rows)
+        while left:
+            for r in srv.poll(64, wait_ms=100):
+                srv.release(r.request_id)
+                left -= 1
+
+    results = {}
+    with ClockSampler(0) as clk:
+        ser, ser_t = make(1)
+        con, con_t = make(args.slots)
+        warm(ser, ser_t)
+        warm(con, con_t)
+        s_sat, s_span = run(ser, ser_t, None, 0)
+        c_sat, c_span = run(con, con_t, None, 100_000)
+        for i in range(len(reqs)):
+            assert s_sat[i][1] == c_sat[i][1], f"request {i}: serial and concurrent counts differ"
+        cap = len(reqs) / s_span  # serial capacity, requests/s
+        rng = np.random.default_rng(args.seed + 77)
+        gaps = rng.exponential(1.0, size=len(reqs))
+        for k, frac in enumerate((0.5, 0.8, 0.95)):
+            arr = np.cumsum(gaps) / (frac * cap)
+            arr -= arr[0]
+            s_p, _ = run(ser, ser_t, arr, 200_000 + 10_000 * k)
+            c_p, _ = run(con, con_t, arr, 300_000 + 10_000 * k)
+            for i in range(len(reqs)):
+                assert s_p[i][1] == c_p[i][1] == s_sat[i][1], f"request {i}: counts differ between runs"
+            lat = lambda d: [v[0] * 1e3 for v in d.values()]
+            results[frac] = {"arrival_rate_rps": round(frac * cap, 2),
+                             "serial_p50_ms": round(_pct(lat(s_p), 50), 3), "serial_p99_ms": round(_pct(lat(s_p), 99), 3),
+                             "served_p50_ms": round(_pct(lat(c_p), 50), 3), "served_p99_ms": round(_pct(lat(c_p), 99), 3)}
+        con.close()
+        ser.close()
+    matches = sum(v[1] for v in s_sat.values())
+    line = {
+        "metric": "served join stream: probe Mtuples/s at saturation, p50/p99 request latency",
+        "value": round(probe_rows / c_span / 1e6, 3), "unit": "Mtuples/s", "n_gpus": 1, "steps": 1,
+        "warmup": 1, "ms_per_step": round(c_span * 1e3, 3), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "int64", "data": "synthetic (generated on the device)",
+        "config": {"workload": "8 resident tables of unique int64 keys (1M,2M,4M,8M,16M,24M,32M,48M rows, one int64 "
+                               "payload); requests pick a table uniformly, probe log-uniform 10K..20M int64 keys at a "
+                               "70% hit rate; 120 GiB admission budget",
+                   "requests": len(reqs), "probe_rows": probe_rows, "matches": matches, "slots": args.slots},
+        "serial_value": round(probe_rows / s_span / 1e6, 3),
+        "throughput_speedup_vs_serial": round(s_span / c_span, 3),
+        "saturated": {"serial_makespan_s": round(s_span, 4), "served_makespan_s": round(c_span, 4),
+                      "serial_p50_ms": round(_pct([v[0] * 1e3 for v in s_sat.values()], 50), 3),
+                      "serial_p99_ms": round(_pct([v[0] * 1e3 for v in s_sat.values()], 99), 3),
+                      "served_p50_ms": round(_pct([v[0] * 1e3 for v in c_sat.values()], 50), 3),
+                      "served_p99_ms": round(_pct([v[0] * 1e3 for v in c_sat.values()], 99), 3)},
+        "poisson": {str(k): v for k, v in results.items()},
+        "clocks": clk.summary(),
     }
     print(json.dumps(line), flush=True)
     return 0
@@ -531,6 +678,8 @@ def main():
         return run_reference(args)
     if args.workload == "batched":
         return run_batched(args)
+    if args.workload == "served":
+        return run_served(args)
     return run_sj(args)
 
 

@@ -299,6 +299,65 @@ SJ_EXPORT sj_status sj_batch_plan_counts(const sj_batch_plan* plan, int64_t* d_c
 
 SJ_EXPORT sj_status sj_batch_plan_destroy(sj_batch_plan* plan, sj_stream_t stream);
 
+/* ---------------------------------------------------------------------------------------------
+ * Serving: resident tables, probe requests admitted continuously against a memory budget
+ * (the BUILD_PROBE pattern, src/op/sirius_physical_hash_join.cpp:1585-1624, with admission in the
+ * manner of exec::admission_control, src/include/exec/admission_control.hpp:39-104).
+ * ------------------------------------------------------------------------------------------- */
+
+typedef struct sj_server sj_server;
+
+typedef struct sj_server_config {
+  int32_t slots;                /* requests on the GPU at once, one CUDA stream each; default 4 */
+  int32_t max_skip;             /* times the queue head may be passed by smaller requests; 8 */
+  int64_t memory_budget_bytes;  /* device bytes for request outputs + scratch; default 120 GiB */
+  int32_t reserved[8];
+} sj_server_config;
+
+/* A finished request. Output buffers are device memory owned by the server until
+ * sj_server_release(request_id); columns are [probe row id, build row id, attached build
+ * payloads...] with `count` valid rows. Times are seconds on one steady clock. */
+typedef struct sj_request_result {
+  uint64_t request_id;
+  int32_t status;   /* sj_status of the request */
+  int32_t table_id;
+  int64_t count;
+  int64_t probe_rows;
+  int32_t* probe_rid;
+  int32_t* build_rid;
+  void* build_payload[8];
+  uint32_t* build_validity[8]; /* NULL where the payload column has no validity */
+  double t_submit;  /* sj_server_submit returned */
+  double t_admit;   /* admitted onto a slot */
+  double t_done;    /* its last GPU operation finished */
+} sj_request_result;
+
+/* Start a server on the current device (its worker thread runs until sj_server_destroy). */
+SJ_EXPORT sj_status sj_server_create(const sj_server_config* config, sj_server** out);
+
+/* Build a resident table (unique keys: DISTINCT layout) with its attached payload columns.
+ * Synchronizes. *table_id receives the table's id. */
+SJ_EXPORT sj_status sj_server_add_table(sj_server* server, const sj_column* key, const sj_column* payload,
+                                        int32_t num_payload, const sj_join_params* params,
+                                        int32_t* table_id);
+
+/* Queue a probe request: INNER join of `probe_key` (device column, valid until the request
+ * completes) with table `table_id`. Returns immediately; the worker admits the request when a slot
+ * is free and its outputs + scratch fit the budget. A request larger than the whole budget fails
+ * with SJ_ERR_BUSY. */
+SJ_EXPORT sj_status sj_server_submit(sj_server* server, int32_t table_id, const sj_column* probe_key,
+                                     uint64_t request_id);
+
+/* Move up to `capacity` finished requests into `out`, waiting up to `wait_ms` for at least one.
+ * Returns the number written (>= 0) or a negative sj_status. */
+SJ_EXPORT int32_t sj_server_poll(sj_server* server, sj_request_result* out, int32_t capacity, int32_t wait_ms);
+
+/* Free a finished request's output buffers (returns their bytes to the budget). */
+SJ_EXPORT sj_status sj_server_release(sj_server* server, uint64_t request_id);
+
+/* Stop the worker after the queued and in-flight requests finish and free everything. */
+SJ_EXPORT sj_status sj_server_destroy(sj_server* server);
+
 /* The one-shot INNER join of sj_inner_join for callers that cannot allocate device memory: code
  * held to a device-memory reservation that is already fully committed (an allocation attempt
  * there would be refused and rescheduled as out-of-memory), latency-critical host threads that

@@ -6,8 +6,8 @@ raises, so a GPU run can never silently take a CPU or library path.
 from __future__ import annotations
 
 import ctypes
-from ctypes import (POINTER, Structure, c_float, c_int32, c_int64, c_size_t, c_uint32, c_void_p, c_char_p,
-                    CFUNCTYPE)
+from ctypes import (POINTER, Structure, c_double, c_float, c_int32, c_int64, c_size_t, c_uint32, c_uint64, c_void_p,
+                    c_char_p, CFUNCTYPE)
 from pathlib import Path
 
 LIB_PATH = Path(__file__).resolve().parent / "libsj.so"
@@ -71,6 +71,18 @@ class SjKernelTime(Structure):
     _fields_ = [("name", c_char_p), ("ms", c_float), ("reserved", c_int32)]
 
 
+class SjServerConfig(Structure):
+    _fields_ = [("slots", c_int32), ("max_skip", c_int32), ("memory_budget_bytes", c_int64),
+                ("reserved", c_int32 * 8)]
+
+
+class SjRequestResult(Structure):
+    _fields_ = [("request_id", c_uint64), ("status", c_int32), ("table_id", c_int32), ("count", c_int64),
+                ("probe_rows", c_int64), ("probe_rid", c_void_p), ("build_rid", c_void_p),
+                ("build_payload", c_void_p * 8), ("build_validity", c_void_p * 8), ("t_submit", c_double),
+                ("t_admit", c_double), ("t_done", c_double)]
+
+
 # (name, restype, argtypes) of every function the header declares.
 _P = POINTER
 SIGNATURES = {
@@ -102,6 +114,12 @@ SIGNATURES = {
     "sj_batch_plan_counts": (c_int32, [c_void_p, c_void_p, c_void_p, c_void_p]),
     "sj_batch_plan_destroy": (c_int32, [c_void_p, c_void_p]),
     "sj_timing_collect": (c_int32, [_P(SjKernelTime), c_int32]),
+    "sj_server_create": (c_int32, [_P(SjServerConfig), _P(c_void_p)]),
+    "sj_server_add_table": (c_int32, [c_void_p, _P(SjColumn), _P(SjColumn), c_int32, _P(SjJoinParams), _P(c_int32)]),
+    "sj_server_submit": (c_int32, [c_void_p, c_int32, _P(SjColumn), c_uint64]),
+    "sj_server_poll": (c_int32, [c_void_p, _P(SjRequestResult), c_int32, c_int32]),
+    "sj_server_release": (c_int32, [c_void_p, c_uint64]),
+    "sj_server_destroy": (c_int32, [c_void_p]),
 }
 
 _lib = None

@@ -139,6 +139,9 @@ sj_status build_table(const sj_column& keys, const sj_column* payload, int32_t n
                       const sj_join_params& p, const Allocator& alloc, cudaStream_t stream, sj_table** out);
 sj_status destroy_table(sj_table* t, cudaStream_t stream);
 
+// Probes of a radix-partitioned table with at least this many rows are partitioned too.
+constexpr int64_t kMinPartitionedProbe = 1 << 16;
+
 struct GatherSpec {
   const sj_column* probe_payload;
   int32_t n_probe_payload;

@@ -732,7 +732,6 @@ static sj_status probe_partitioned(const sj_table* t, const sj_column& p, Gather
 }
 
 // Probes of at least this many rows into a partitioned table take the partitioned path.
-constexpr int64_t kMinPartitionedProbe = 1 << 16;
 
 sj_status probe_gather(const sj_table* t, const sj_column& p, const GatherSpec& gs, const Allocator& alloc,
                        cudaStream_t s, int64_t* d_count) {

@@ -182,3 +182,62 @@ def served_request(seed: int, i: int, table_keys: np.ndarray, t: int, n_probe: i
     keys = np.concatenate([hits, misses])
     r.shuffle(keys)
     return keys, n_hit
+
+
+# ---- the served workload generated on the device (same key functions as above) ----
+
+def _srl(x, s: int):
+    """Logical right shift of int64 tensor bits."""
+    return (x >> s) & ((1 << (64 - s)) - 1)
+
+
+def mix64_torch(x):
+    """mix64 on an int64 torch tensor (bit pattern as uint64; multiplication wraps)."""
+    m1 = int(_M1) - (1 << 64)
+    m2 = int(_M2) - (1 << 64)
+    x = x ^ _srl(x, 30)
+    x = x * m1
+    x = x ^ _srl(x, 27)
+    x = x * m2
+    return x ^ _srl(x, 31)
+
+
+def _served_base(seed: int, t: int) -> int:
+    b = ((t + 1) << 40) + (seed % 256) * (1 << 56)
+    return b - (1 << 64) if b >= 1 << 63 else b
+
+
+def served_table_device(seed: int, t: int, n_rows: int, device):
+    """served_table(seed, t, n_rows) generated on `device` (identical keys; payload from torch's
+    generator)."""
+    import torch
+    idx = torch.arange(n_rows, dtype=torch.int64, device=device) + _served_base(seed, t)
+    g = torch.Generator(device=device)
+    g.manual_seed(seed * 7919 + t)
+    payload = torch.randint(-2**62, 2**62, (n_rows,), dtype=torch.int64, device=device, generator=g)
+    return mix64_torch(idx), payload
+
+
+def served_probe_pool(seed: int, t: int, table_keys, n_pool: int, hit_rate: float = 0.7):
+    """A shuffled pool of probe keys for table t: hit_rate of them drawn from the table's keys, the
+    rest absent from it (mix64 of indices past the table's range). A request of n rows probes a
+    random window of the pool."""
+    import torch
+    dev = table_keys.device
+    g = torch.Generator(device=dev)
+    g.manual_seed(seed * 104729 + t)
+    n_hit = int(round(n_pool * hit_rate))
+    hits = table_keys[torch.randint(0, table_keys.numel(), (n_hit,), device=dev, generator=g)]
+    miss_idx = table_keys.numel() + torch.randint(0, 1 << 30, (n_pool - n_hit,), device=dev, generator=g)
+    misses = mix64_torch(miss_idx + _served_base(seed, t))
+    keys = torch.cat([hits, misses])
+    return keys[torch.randperm(n_pool, device=dev, generator=g)]
+
+
+def served_requests(seed: int, n_requests: int, n_tables: int = 8, lo: float = 1e4, hi: float = 2e7):
+    """(table, probe rows, window seed) per request: table uniform, size log-uniform [lo, hi]."""
+    r = _rng(seed, 6000)
+    tables = r.integers(0, n_tables, size=n_requests)
+    sizes = np.floor(np.exp(r.uniform(np.log(lo), np.log(hi), size=n_requests))).astype(np.int64)
+    starts = r.random(n_requests)
+    return tables, sizes, starts

@@ -56,6 +56,10 @@ int main(void) {
          sizeof(sj_join_params), sizeof(sj_table_info));
   printf("%zu %zu %zu\n", offsetof(sj_column, num_rows), offsetof(sj_join_params, ctas_per_sm),
          offsetof(sj_table_info, max_group));
+  printf("%zu %zu %zu %zu %zu\n", sizeof(sj_batch_join), sizeof(sj_batch_params), sizeof(sj_kernel_time),
+         sizeof(sj_server_config), sizeof(sj_request_result));
+  printf("%zu %zu %zu\n", offsetof(sj_batch_join, capacity), offsetof(sj_request_result, build_validity),
+         offsetof(sj_request_result, t_done));
   return 0;
 }
 ''')
@@ -64,7 +68,11 @@ int main(void) {
     got = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()
     exp = [ctypes.sizeof(_lib.SjColumn), ctypes.sizeof(_lib.SjMutColumn), ctypes.sizeof(_lib.SjAlloc),
            ctypes.sizeof(_lib.SjJoinParams), ctypes.sizeof(_lib.SjTableInfo),
-           _lib.SjColumn.num_rows.offset, _lib.SjJoinParams.ctas_per_sm.offset, _lib.SjTableInfo.max_group.offset]
+           _lib.SjColumn.num_rows.offset, _lib.SjJoinParams.ctas_per_sm.offset, _lib.SjTableInfo.max_group.offset,
+           ctypes.sizeof(_lib.SjBatchJoin), ctypes.sizeof(_lib.SjBatchParams), ctypes.sizeof(_lib.SjKernelTime),
+           ctypes.sizeof(_lib.SjServerConfig), ctypes.sizeof(_lib.SjRequestResult),
+           _lib.SjBatchJoin.capacity.offset, _lib.SjRequestResult.build_validity.offset,
+           _lib.SjRequestResult.t_done.offset]
     assert [int(x) for x in got] == exp
 
 

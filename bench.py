@@ -56,11 +56,14 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--partition-bits", type=int, default=0)
     ap.add_argument("--aggregation", type=int, default=0)
+    ap.add_argument("--probe-kernel", type=int, default=0, help="0 auto, 1 staged write-out, 2 direct write-out")
+    ap.add_argument("--rows-per-lane", type=int, default=0)
     ap.add_argument("--workload", default="large", choices=["large", "batched", "served"])
     ap.add_argument("--autotune", action="store_true", help="batched: choose launch parameters by the autotuner")
     ap.add_argument("--requests", type=int, default=2000)
     ap.add_argument("--slots", type=int, default=4)
     ap.add_argument("--served-max-rows", type=int, default=20_000_000)
+    ap.add_argument("--reserve-gib", type=int, default=16, help="served: device memory each server pool takes up front")
     ap.add_argument("--joins", type=int, default=4096)
     ap.add_argument("--wave-probe-rows", type=int, default=1_500_000_000)
     ap.add_argument("--block-size", type=int, default=0)
@@ -259,7 +262,8 @@ def run_sj(args):
     for i in range(3):
         torch.cuda.synchronize()
         ev0.record()
-        tb = J.HashTable(bk, attach=bp, partition_bits=args.partition_bits, aggregation=args.aggregation)
+        tb = J.HashTable(bk, attach=bp, partition_bits=args.partition_bits, aggregation=args.aggregation,
+                         probe_kernel=args.probe_kernel, rows_per_lane=args.rows_per_lane)
         ev1.record()
         torch.cuda.synchronize()
         t_build.append(ev0.elapsed_time(ev1))
@@ -334,7 +338,8 @@ def run_sj(args):
             d_pk.copy_(h_pk, non_blocking=True)
             for d, h in zip(d_bp + d_pp, h_bp + h_pp):
                 d.copy_(h, non_blocking=True)
-            with J.HashTable(d_bk, attach=d_bp, partition_bits=args.partition_bits) as tt:
+            with J.HashTable(d_bk, attach=d_bp, partition_bits=args.partition_bits, probe_kernel=args.probe_kernel,
+                             rows_per_lane=args.rows_per_lane) as tt:
                 tt.probe_gather(d_pk, None, d_pp, attached=True, capacity=args.n_probe, out=out, d_count=d_count,
                                 sync=False)
                 srcs = [out.probe_rid, out.build_rid] + out.probe_payload + out.build_payload
@@ -575,7 +580,7 @@ def run_served(args):
     torch.cuda.synchronize()
 
     def make(slots):
-        srv = S.JoinServer(slots=slots, memory_budget_bytes=120 << 30)
+        srv = S.JoinServer(slots=slots, memory_budget_bytes=120 << 30, reserve_bytes=args.reserve_gib << 30)
         tids = [srv.add_table(k, attach=[p]) for k, p in tables]
         return srv, tids
 
@@ -612,22 +617,13 @@ def run_served(args):
         makespan = max(v[3] for v in got.values()) - min(v[2] for v in got.values())
         return got, makespan
 
-    def warm(srv, tids):
-        for t in range(len(rows)):
-            for m in (10_000, 1_000_000):
-                srv.submit(tids[t], pools[t][:m], 10**9 + t * 10 + (m > 10_000), sync=False)
-        left = 2 * len(rows)
-        while left:
-            for r in srv.poll(64, wait_ms=100):
-                srv.release(r.request_id)
-                left -= 1
-
     results = {}
     with ClockSampler(0) as clk:
         ser, ser_t = make(1)
         con, con_t = make(args.slots)
-        warm(ser, ser_t)
-        warm(con, con_t)
+        # warm-up: one untimed saturated pass per server (kernels loaded, memory pools grown)
+        run(ser, ser_t, None, 10_000_000)
+        run(con, con_t, None, 20_000_000)
         s_sat, s_span = run(ser, ser_t, None, 0)
         c_sat, c_span = run(con, con_t, None, 100_000)
         for i in range(len(reqs)):
@@ -657,7 +653,8 @@ def run_served(args):
         "config": {"workload": "8 resident tables of unique int64 keys (1M,2M,4M,8M,16M,24M,32M,48M rows, one int64 "
                                "payload); requests pick a table uniformly, probe log-uniform 10K..20M int64 keys at a "
                                "70% hit rate; 120 GiB admission budget",
-                   "requests": len(reqs), "probe_rows": probe_rows, "matches": matches, "slots": args.slots},
+                   "requests": len(reqs), "probe_rows": probe_rows, "matches": matches, "slots": args.slots,
+                   "pool_reserve_gib": args.reserve_gib},
         "serial_value": round(probe_rows / s_span / 1e6, 3),
         "throughput_speedup_vs_serial": round(s_span / c_span, 3),
         "saturated": {"serial_makespan_s": round(s_span, 4), "served_makespan_s": round(c_span, 4),

@@ -131,6 +131,17 @@ typedef enum sj_slot_kind {
 typedef enum sj_aggregation { SJ_AGG_AUTO = 0, SJ_AGG_WARP = 1, SJ_AGG_CTA = 2 } sj_aggregation;
 
 /* Tunables. Zero-initialised fields take defaults (sj_default_params fills them in). */
+/* How a DISTINCT probe writes its output rows. DIRECT: lanes write their own matches at
+ * positions ranked by warp ballots (no shared-memory staging); it serves outputs of row ids, up
+ * to 2 probe payloads and up to 3 build payloads of 4 or 8 bytes without NULLs (attached build
+ * payloads: 8-byte fields). STAGED: matches are staged per warp in shared memory and written column
+ * by column; it serves every output shape. AUTO takes DIRECT where it applies. */
+typedef enum sj_probe_kernel {
+  SJ_PROBE_KERNEL_AUTO = 0,
+  SJ_PROBE_KERNEL_STAGED = 1,
+  SJ_PROBE_KERNEL_DIRECT = 2
+} sj_probe_kernel;
+
 typedef struct sj_join_params {
   int32_t layout;           /* sj_layout */
   int32_t null_equality;    /* sj_null_equality */
@@ -143,7 +154,9 @@ typedef struct sj_join_params {
   int32_t force_wide;       /* 1 = use SJ_SLOT_WIDE128 even when the packed encoding fits */
   int32_t ctas_per_sm;      /* grid = ctas_per_sm * SM count for grid-stride kernels; default 4 */
   int32_t aggregation;      /* sj_aggregation: how probe matches reserve output positions */
-  int32_t reserved[7];
+  int32_t probe_kernel;     /* sj_probe_kernel: write-out of DISTINCT probes; default AUTO */
+  int32_t rows_per_lane;    /* probe rows per lane and tile of the direct kernel: 2 or 4; 0 = 2 */
+  int32_t reserved[5];
 } sj_join_params;
 
 typedef struct sj_table sj_table;
@@ -311,7 +324,9 @@ typedef struct sj_server_config {
   int32_t slots;                /* requests on the GPU at once, one CUDA stream each; default 4 */
   int32_t max_skip;             /* times the queue head may be passed by smaller requests; 8 */
   int64_t memory_budget_bytes;  /* device bytes for request outputs + scratch; default 120 GiB */
-  int32_t reserved[8];
+  int64_t reserve_bytes;        /* device memory the server's pool takes up front and keeps, so
+                                   requests are served without growing it; default 0 */
+  int32_t reserved[6];
 } sj_server_config;
 
 /* A finished request. Output buffers are device memory owned by the server until

@@ -22,6 +22,7 @@ SJ_LAYOUT_AUTO, SJ_LAYOUT_DISTINCT, SJ_LAYOUT_GROUPED = 0, 1, 2
 SJ_NULLS_UNEQUAL, SJ_NULLS_EQUAL = 0, 1
 SJ_SLOT_PACKED64, SJ_SLOT_WIDE128 = 0, 1
 SJ_AGG_AUTO, SJ_AGG_WARP, SJ_AGG_CTA = 0, 1, 2
+SJ_PROBE_KERNEL_AUTO, SJ_PROBE_KERNEL_STAGED, SJ_PROBE_KERNEL_DIRECT = 0, 1, 2
 
 
 class SjColumn(Structure):
@@ -45,7 +46,7 @@ class SjJoinParams(Structure):
     _fields_ = [("layout", c_int32), ("null_equality", c_int32), ("load_factor", c_float),
                 ("block_size", c_int32), ("group_width", c_int32), ("partition_bits", c_int32),
                 ("force_wide", c_int32), ("ctas_per_sm", c_int32), ("aggregation", c_int32),
-                ("reserved", c_int32 * 7)]
+                ("probe_kernel", c_int32), ("rows_per_lane", c_int32), ("reserved", c_int32 * 5)]
 
 
 class SjTableInfo(Structure):
@@ -73,7 +74,7 @@ class SjKernelTime(Structure):
 
 class SjServerConfig(Structure):
     _fields_ = [("slots", c_int32), ("max_skip", c_int32), ("memory_budget_bytes", c_int64),
-                ("reserved", c_int32 * 8)]
+                ("reserve_bytes", c_int64), ("reserved", c_int32 * 6)]
 
 
 class SjRequestResult(Structure):

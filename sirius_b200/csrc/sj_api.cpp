@@ -168,6 +168,8 @@ static sj_join_params resolve(const sj_join_params* p) {
   r.force_wide = p->force_wide;
   if (p->ctas_per_sm > 0) r.ctas_per_sm = p->ctas_per_sm;
   r.aggregation = p->aggregation;
+  r.probe_kernel = p->probe_kernel;
+  r.rows_per_lane = p->rows_per_lane;
   return r;
 }
 

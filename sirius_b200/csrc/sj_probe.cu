@@ -25,6 +25,7 @@
 #include "sj_device.cuh"
 #include "sj_internal.h"
 #include "sj_partition.cuh"
+#include "sj_probe_direct.h"
 #include "sj_scan.cuh"
 
 namespace sj {
@@ -726,7 +727,7 @@ static sj_status probe_partitioned(const sj_table* t, const sj_column& p, Gather
   for (int c = 0; c < g.n_pin; ++c)
     g.pin[c] = PayloadIn{pd.pay[c], nullptr, pd.valid8[c], 0, g.pin[c].width, g.pin[c].width, 1, 0};
   const sj_column pk{pd.keys, nullptr, 0, n, t->key_type, 0};
-  dispatch_distinct<false>(t, pk, d_total, g, s);
+  if (!probe_direct(t, pk, d_total, g, s)) dispatch_distinct<false>(t, pk, d_total, g, s);
   SJ_CUDA_TRY(cudaGetLastError());
   return SJ_OK;
 }
@@ -749,7 +750,7 @@ sj_status probe_gather(const sj_table* t, const sj_column& p, const GatherSpec& 
 
   if (t->layout == SJ_LAYOUT_DISTINCT) {
     if (t->pbits > 0 && p.num_rows >= kMinPartitionedProbe) return probe_partitioned(t, p, g, alloc, s);
-    dispatch_distinct<false>(t, p, nullptr, g, s);
+    if (!probe_direct(t, p, nullptr, g, s)) dispatch_distinct<false>(t, p, nullptr, g, s);
     SJ_CUDA_TRY(cudaGetLastError());
     return SJ_OK;
   }

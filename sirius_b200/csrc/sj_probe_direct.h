@@ -1,0 +1,41 @@
+// The direct write-out DISTINCT probe (sj_probe_direct.cu): its argument block and entry point.
+#pragma once
+
+#include "sj_device.cuh"
+#include "sj_internal.h"
+
+namespace sj {
+
+constexpr int kDirectMaxProbePayload = 2;
+constexpr int kDirectMaxBuildPayload = 3;
+
+struct DirectArgs {
+  int32_t* out_prid;
+  int32_t* out_brid;
+  const int32_t* prid_map;  // probe array index -> probe row id (partitioned probe), or NULL
+  const int32_t* brid_map;  // table position -> build row id at brid_map + pos * brid_stride bytes
+  int32_t brid_stride;
+  int32_t bin_by_pos;       // build payload element index: table position (1) or build row id (0)
+  const void* rec;          // row store (record = [row id | pad | 8-byte fields]) or NULL
+  int32_t rec_stride;
+  int32_t n_pin, n_bin;
+  const void* pin[kDirectMaxProbePayload];
+  int32_t pin_w[kDirectMaxProbePayload];
+  void* pout[kDirectMaxProbePayload];
+  const void* bin[kDirectMaxBuildPayload];
+  int32_t bin_stride[kDirectMaxBuildPayload];
+  int32_t bin_w[kDirectMaxBuildPayload];
+  void* bout[kDirectMaxBuildPayload];
+  int64_t capacity;
+  unsigned long long* d_count;
+};
+
+// Fills `a` from a general gather description; false when the output shape needs the staged
+// kernel (NULL payloads, 1/2-byte payloads, too many columns, other record layouts).
+bool direct_args(const GatherArgs& g, DirectArgs& a);
+
+// Launches the direct probe of DISTINCT table `t` when the shape allows and the table's
+// parameters do not ask for the staged kernel; returns false (nothing launched) otherwise.
+bool probe_direct(const sj_table* t, const sj_column& p, const int64_t* d_n, const GatherArgs& g, cudaStream_t s);
+
+}  // namespace sj

@@ -81,6 +81,7 @@ struct sj_server {
   sj_server_config cfg{};
   int device = 0;
   cudaMemPool_t pool = nullptr;
+  cudaStream_t release_stream = nullptr;  // frees of released outputs: never waits on a request
   std::vector<sj::SrvTable> tables;
   std::vector<sj::SrvSlot> slots;
   std::deque<sj::SrvReq*> pending;
@@ -280,6 +281,7 @@ SJ_EXPORT sj_status sj_server_create(const sj_server_config* config, sj_server**
     if (config->slots > 0) S->cfg.slots = config->slots;
     if (config->max_skip > 0) S->cfg.max_skip = config->max_skip;
     if (config->memory_budget_bytes > 0) S->cfg.memory_budget_bytes = config->memory_budget_bytes;
+    if (config->reserve_bytes > 0) S->cfg.reserve_bytes = std::min(config->reserve_bytes, S->cfg.memory_budget_bytes);
   }
   if (S->cfg.slots > 64) {
     delete S;
@@ -296,6 +298,27 @@ SJ_EXPORT sj_status sj_server_create(const sj_server_config* config, sj_server**
   }
   uint64_t thr = ~0ull;
   cudaMemPoolSetAttribute(S->pool, cudaMemPoolAttrReleaseThreshold, &thr);
+  // No hidden cross-stream waits: a request's allocation must not reuse a block whose free is
+  // still queued behind another slot's request (that would make it wait for that request).
+  int no = 0;
+  cudaMemPoolSetAttribute(S->pool, cudaMemPoolReuseAllowInternalDependencies, &no);
+  if (cudaStreamCreateWithFlags(&S->release_stream, cudaStreamNonBlocking) != cudaSuccess) {
+    cudaMemPoolDestroy(S->pool);
+    delete S;
+    return set_error(SJ_ERR_DEVICE, "creating the server's streams failed");
+  }
+  if (S->cfg.reserve_bytes > 0) {
+    void* p = nullptr;
+    if (cudaMallocFromPoolAsync(&p, (size_t)S->cfg.reserve_bytes, S->pool, S->release_stream) != cudaSuccess) {
+      cudaGetLastError();
+      cudaStreamDestroy(S->release_stream);
+      cudaMemPoolDestroy(S->pool);
+      delete S;
+      return set_error(SJ_ERR_OOM, "cannot reserve the server's memory up front");
+    }
+    cudaFreeAsync(p, S->release_stream);
+    cudaStreamSynchronize(S->release_stream);
+  }
   S->slots.resize(S->cfg.slots);
   for (SrvSlot& sl : S->slots) {
     if (cudaStreamCreateWithFlags(&sl.stream, cudaStreamNonBlocking) != cudaSuccess ||
@@ -411,7 +434,7 @@ SJ_EXPORT sj_status sj_server_release(sj_server* S, uint64_t id) {
     if (it == S->polled.end()) return set_error(SJ_ERR_INVALID, "unknown or unpolled request id");
     r = it->second;
     S->polled.erase(it);
-    free_outputs(S, r, S->slots[0].stream);
+    free_outputs(S, r, S->release_stream);
     S->in_use -= r->out_bytes;
   }
   delete r;
@@ -428,7 +451,7 @@ SJ_EXPORT sj_status sj_server_destroy(sj_server* S) {
   S->cv_work.notify_all();
   if (S->worker.joinable()) S->worker.join();
   cudaSetDevice(S->device);
-  cudaStream_t s0 = S->slots.empty() ? nullptr : S->slots[0].stream;
+  cudaStream_t s0 = S->release_stream;
   for (auto& kv : S->polled) {
     free_outputs(S, kv.second, s0);
     delete kv.second;
@@ -446,6 +469,7 @@ SJ_EXPORT sj_status sj_server_destroy(sj_server* S) {
   }
   for (SrvTable& T : S->tables) destroy_table(T.t, nullptr);
   cudaDeviceSynchronize();
+  if (S->release_stream) cudaStreamDestroy(S->release_stream);
   if (S->pool) cudaMemPoolDestroy(S->pool);
   delete S;
   return SJ_OK;

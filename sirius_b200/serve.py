@@ -64,11 +64,13 @@ class RequestResult:
 class JoinServer:
     """Resident tables + continuous batching of probe requests (``sj_server_create``)."""
 
-    def __init__(self, slots: int = 4, max_skip: int = 8, memory_budget_bytes: int = 120 << 30, device=None):
+    def __init__(self, slots: int = 4, max_skip: int = 8, memory_budget_bytes: int = 120 << 30,
+                 reserve_bytes: int = 0, device=None):
         self._lib = L.load()
         self.device = torch.device("cuda", torch.cuda.current_device()) if device is None else torch.device(device)
         cfg = L.SjServerConfig()
         cfg.slots, cfg.max_skip, cfg.memory_budget_bytes = slots, max_skip, memory_budget_bytes
+        cfg.reserve_bytes = reserve_bytes
         self._h = ctypes.c_void_p()
         with torch.cuda.device(self.device):
             L.check(self._lib.sj_server_create(ctypes.byref(cfg), ctypes.byref(self._h)), "sj_server_create")

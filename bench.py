@@ -58,6 +58,7 @@ def parse():
     ap.add_argument("--aggregation", type=int, default=0)
     ap.add_argument("--probe-kernel", type=int, default=0, help="0 auto, 1 staged write-out, 2 direct write-out")
     ap.add_argument("--rows-per-lane", type=int, default=0)
+    ap.add_argument("--ctas-per-sm", type=int, default=0)
     ap.add_argument("--workload", default="large", choices=["large", "batched", "served"])
     ap.add_argument("--autotune", action="store_true", help="batched: choose launch parameters by the autotuner")
     ap.add_argument("--requests", type=int, default=2000)
@@ -263,7 +264,8 @@ def run_sj(args):
         torch.cuda.synchronize()
         ev0.record()
         tb = J.HashTable(bk, attach=bp, partition_bits=args.partition_bits, aggregation=args.aggregation,
-                         probe_kernel=args.probe_kernel, rows_per_lane=args.rows_per_lane)
+                         probe_kernel=args.probe_kernel, rows_per_lane=args.rows_per_lane,
+                         ctas_per_sm=args.ctas_per_sm)
         ev1.record()
         torch.cuda.synchronize()
         t_build.append(ev0.elapsed_time(ev1))

@@ -131,15 +131,18 @@ typedef enum sj_slot_kind {
 typedef enum sj_aggregation { SJ_AGG_AUTO = 0, SJ_AGG_WARP = 1, SJ_AGG_CTA = 2 } sj_aggregation;
 
 /* Tunables. Zero-initialised fields take defaults (sj_default_params fills them in). */
-/* How a DISTINCT probe writes its output rows. DIRECT: lanes write their own matches at
- * positions ranked by warp ballots (no shared-memory staging); it serves outputs of row ids, up
- * to 2 probe payloads and up to 3 build payloads of 4 or 8 bytes without NULLs (attached build
- * payloads: 8-byte fields). STAGED: matches are staged per warp in shared memory and written column
- * by column; it serves every output shape. AUTO takes DIRECT where it applies. */
+/* How a DISTINCT probe reads its rows and writes its output. DIRECT: lanes write their own
+ * matches at positions ranked by warp ballots (no shared-memory staging of matches); it serves
+ * outputs of row ids, up to 2 probe payloads and up to 3 build payloads of 4 or 8 bytes without
+ * NULLs (attached build payloads: 8-byte fields). DIRECT_TMA: DIRECT with the probe rows (keys,
+ * payloads) bulk-copied into shared memory two tiles ahead by the TMA engine; needs 16-byte
+ * aligned probe columns. STAGED: matches are staged per warp in shared memory and written column
+ * by column; it serves every output shape. AUTO takes DIRECT where it applies, else STAGED. */
 typedef enum sj_probe_kernel {
   SJ_PROBE_KERNEL_AUTO = 0,
   SJ_PROBE_KERNEL_STAGED = 1,
-  SJ_PROBE_KERNEL_DIRECT = 2
+  SJ_PROBE_KERNEL_DIRECT = 2,
+  SJ_PROBE_KERNEL_DIRECT_TMA = 3
 } sj_probe_kernel;
 
 typedef struct sj_join_params {

@@ -22,7 +22,7 @@ SJ_LAYOUT_AUTO, SJ_LAYOUT_DISTINCT, SJ_LAYOUT_GROUPED = 0, 1, 2
 SJ_NULLS_UNEQUAL, SJ_NULLS_EQUAL = 0, 1
 SJ_SLOT_PACKED64, SJ_SLOT_WIDE128 = 0, 1
 SJ_AGG_AUTO, SJ_AGG_WARP, SJ_AGG_CTA = 0, 1, 2
-SJ_PROBE_KERNEL_AUTO, SJ_PROBE_KERNEL_STAGED, SJ_PROBE_KERNEL_DIRECT = 0, 1, 2
+SJ_PROBE_KERNEL_AUTO, SJ_PROBE_KERNEL_STAGED, SJ_PROBE_KERNEL_DIRECT, SJ_PROBE_KERNEL_DIRECT_TMA = 0, 1, 2, 3
 
 
 class SjColumn(Structure):

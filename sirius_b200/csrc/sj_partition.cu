@@ -30,33 +30,48 @@ __device__ __forceinline__ int partition_of(uint64_t kb, int pbits) {
 }
 
 template <typename K>
+__device__ __forceinline__ void hist_load4(const K* keys, int64_t i0, int64_t hi, bool vec, K (&k)[4]) {
+  if (vec && i0 + 4 <= hi) {
+    if (sizeof(K) == 4) {
+      const int4 x = __ldcs(reinterpret_cast<const int4*>(keys + i0));
+      k[0] = (K)x.x; k[1] = (K)x.y; k[2] = (K)x.z; k[3] = (K)x.w;
+    } else {
+      const longlong2 x = __ldcs(reinterpret_cast<const longlong2*>(keys + i0));
+      const longlong2 y = __ldcs(reinterpret_cast<const longlong2*>(keys + i0) + 1);
+      k[0] = (K)x.x; k[1] = (K)x.y; k[2] = (K)y.x; k[3] = (K)y.y;
+    }
+  } else {
+#pragma unroll
+    for (int j = 0; j < 4; ++j) k[j] = i0 + j < hi ? __ldcs(keys + i0 + j) : (K)0;
+  }
+}
+
+// Histogram pass: each thread loads 4 groups of 4 consecutive keys (16-byte loads) per step, all
+// before counting them, so 8 (int64) or 4 (int32) vector loads per thread are in flight.
+template <typename K>
 __global__ void __launch_bounds__(kPartThreads) part_hist_kernel(PartSrc s, int pbits, int64_t chunk, bool vec,
                                                                  int32_t* hist) {
   extern __shared__ int32_t h[];
+  constexpr int kGroups = 4;
   const int P = 1 << pbits;
   for (int p = threadIdx.x; p < P; p += blockDim.x) h[p] = 0;
   __syncthreads();
   const int64_t lo = (int64_t)blockIdx.x * chunk;
   const int64_t hi = lo + chunk < s.n ? lo + chunk : s.n;
   const K* keys = static_cast<const K*>(s.keys);
-  for (int64_t i0 = lo + (int64_t)threadIdx.x * 4; i0 < hi; i0 += (int64_t)blockDim.x * 4) {
-    K k[4];
-    if (vec && i0 + 4 <= hi) {
-      if (sizeof(K) == 4) {
-        const int4 x = __ldcs(reinterpret_cast<const int4*>(keys + i0));
-        k[0] = (K)x.x; k[1] = (K)x.y; k[2] = (K)x.z; k[3] = (K)x.w;
-      } else {
-        const longlong2 x = __ldcs(reinterpret_cast<const longlong2*>(keys + i0));
-        const longlong2 y = __ldcs(reinterpret_cast<const longlong2*>(keys + i0) + 1);
-        k[0] = (K)x.x; k[1] = (K)x.y; k[2] = (K)y.x; k[3] = (K)y.y;
-      }
-    } else {
+  const int64_t step = (int64_t)blockDim.x * 4;
+  for (int64_t base = lo; base < hi; base += step * kGroups) {
+    K k[kGroups][4];
 #pragma unroll
-      for (int j = 0; j < 4; ++j) k[j] = i0 + j < hi ? __ldcs(keys + i0 + j) : (K)0;
+    for (int g = 0; g < kGroups; ++g) hist_load4<K>(keys, base + g * step + (int64_t)threadIdx.x * 4, hi, vec, k[g]);
+#pragma unroll
+    for (int g = 0; g < kGroups; ++g) {
+      const int64_t i0 = base + g * step + (int64_t)threadIdx.x * 4;
+#pragma unroll
+      for (int j = 0; j < 4; ++j)
+        if (i0 + j < hi && bit_valid(s.kvalid, s.kvoff, i0 + j))
+          atomicAdd(&h[partition_of(key_u64<K>(k[g][j]), pbits)], 1);
     }
-#pragma unroll
-    for (int j = 0; j < 4; ++j)
-      if (i0 + j < hi && bit_valid(s.kvalid, s.kvoff, i0 + j)) atomicAdd(&h[partition_of(key_u64<K>(k[j]), pbits)], 1);
   }
   __syncthreads();
   for (int p = threadIdx.x; p < P; p += blockDim.x) hist[(int64_t)p * gridDim.x + blockIdx.x] = h[p];
@@ -210,7 +225,211 @@ __global__ void __launch_bounds__(kPartThreads) part_scatter_kernel(PartSrc s, i
   }
 }
 
+// Scatter pass for plain outputs (no row store) with at most 2 payload columns of 4 or 8 bytes
+// without NULLs — the probe side's shape. Each thread holds its 8 rows of a tile (key, payloads)
+// in registers, so all 8-24 loads are in flight at once; the tile is ranked and counting-sorted in
+// shared memory as above (payloads placed directly at their sorted slot), and the loads of the
+// NEXT tile are issued before this tile's runs are written out, so DRAM reads overlap the writes.
+constexpr int kFastMaxPay = 2;
+
+struct FastSmem {
+  size_t cur, tcnt, toff, key, rid, part, pay[kFastMaxPay], total;
+};
+
+static FastSmem fast_smem(int pbits, int kw, int n_pay) {
+  const size_t P = (size_t)1 << pbits;
+  FastSmem m{};
+  size_t o = 0;
+  auto take = [&](size_t b) {
+    size_t r = o;
+    o += (b + 15) & ~(size_t)15;
+    return r;
+  };
+  m.cur = take(P * 8);
+  m.tcnt = take(P * 4);
+  m.toff = take(P * 4);
+  m.key = take((size_t)kTile * kw);
+  m.rid = take((size_t)kTile * 4);
+  m.part = take((size_t)kTile * 2);
+  for (int c = 0; c < n_pay; ++c) m.pay[c] = take((size_t)kTile * 8);
+  m.total = o;
+  return m;
+}
+
+static bool fast_scatter_ok(const PartSrc& s, const PartDst& d) {
+  if (d.stride != 0 || s.n_pay > kFastMaxPay) return false;
+  for (int c = 0; c < s.n_pay; ++c)
+    if (s.pay[c].valid || s.pay[c].valid8 || (s.pay[c].width != 4 && s.pay[c].width != 8) ||
+        s.pay[c].stride != s.pay[c].width || d.valid8[c])
+      return false;
+  return true;
+}
+
+template <typename K, int NP>
+__device__ __forceinline__ void fast_load_tile(const PartSrc& s, int64_t t0, int64_t hi, K (&kk)[kTileRowsPerThread],
+                                               uint64_t (&pv)[kFastMaxPay][kTileRowsPerThread], uint32_t& live) {
+  const K* keys = static_cast<const K*>(s.keys);
+  live = 0;
+#pragma unroll
+  for (int j = 0; j < kTileRowsPerThread; ++j) {
+    const int64_t i = t0 + j * kPartThreads + threadIdx.x;
+    kk[j] = 0;
+#pragma unroll
+    for (int c = 0; c < kFastMaxPay; ++c) pv[c][j] = 0;
+    if (i < hi) {
+      kk[j] = __ldcs(keys + i);
+#pragma unroll
+      for (int c = 0; c < NP; ++c)
+        pv[c][j] = s.pay[c].width == 8 ? __ldcs(static_cast<const unsigned long long*>(s.pay[c].data) + i)
+                                       : (uint64_t)__ldcs(static_cast<const unsigned int*>(s.pay[c].data) + i);
+      if (bit_valid(s.kvalid, s.kvoff, i)) live |= 1u << j;
+    }
+  }
+}
+
+template <typename K, int NP>
+__global__ void __launch_bounds__(kPartThreads, 3) part_scatter_fast_kernel(PartSrc s, int pbits, int64_t chunk,
+                                                                         const int64_t* __restrict__ off, PartDst d,
+                                                                         FastSmem m) {
+  extern __shared__ __align__(16) unsigned char sm[];
+  unsigned long long* cur = reinterpret_cast<unsigned long long*>(sm + m.cur);
+  unsigned int* tcnt = reinterpret_cast<unsigned int*>(sm + m.tcnt);
+  unsigned int* toff = reinterpret_cast<unsigned int*>(sm + m.toff);
+  K* skey = reinterpret_cast<K*>(sm + m.key);
+  int32_t* srid = reinterpret_cast<int32_t*>(sm + m.rid);
+  uint16_t* spart = reinterpret_cast<uint16_t*>(sm + m.part);
+  __shared__ unsigned int s_wsum[kPartThreads / 32];
+  const int P = 1 << pbits;
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  for (int p = tid; p < P; p += kPartThreads) cur[p] = (unsigned long long)off[(int64_t)p * gridDim.x + blockIdx.x];
+  const int64_t lo = (int64_t)blockIdx.x * chunk;
+  const int64_t hi = lo + chunk < s.n ? lo + chunk : s.n;
+  K* okeys = static_cast<K*>(d.keys);
+  K kk[kTileRowsPerThread];
+  uint64_t pv[kFastMaxPay][kTileRowsPerThread];
+  uint32_t live = 0;
+  if (lo < hi) fast_load_tile<K, NP>(s, lo, hi, kk, pv, live);
+  for (int64_t t0 = lo; t0 < hi; t0 += kTile) {
+    for (int p = tid; p < P; p += kPartThreads) tcnt[p] = 0;
+    __syncthreads();
+    // 1. partition and rank within the tile's partition
+    int pr[kTileRowsPerThread];
+    unsigned rank[kTileRowsPerThread];
+#pragma unroll
+    for (int j = 0; j < kTileRowsPerThread; ++j) {
+      pr[j] = (live >> j & 1u) ? partition_of(key_u64<K>(kk[j]), pbits) : -1;
+      const unsigned peers = __match_any_sync(kFullMask, pr[j]);
+      const int leader = __ffs(peers) - 1;
+      unsigned base = 0;
+      if (pr[j] >= 0 && lane == leader) base = atomicAdd(&tcnt[pr[j]], (unsigned)__popc(peers));
+      base = __shfl_sync(kFullMask, base, leader);
+      rank[j] = base + __popc(peers & ((1u << lane) - 1));
+    }
+    __syncthreads();
+    // 2. exclusive scan of the tile histogram
+    constexpr int kBinsPerThread = (1 << kMaxPartitionBits) / kPartThreads;
+    unsigned v[kBinsPerThread], acc = 0;
+#pragma unroll
+    for (int q = 0; q < kBinsPerThread; ++q) {
+      const int p = tid * kBinsPerThread + q;
+      v[q] = p < P ? tcnt[p] : 0;
+      acc += v[q];
+    }
+    unsigned incl = acc;
+#pragma unroll
+    for (int dd = 1; dd < 32; dd <<= 1) {
+      const unsigned o = __shfl_up_sync(kFullMask, incl, dd);
+      if (lane >= dd) incl += o;
+    }
+    if (lane == 31) s_wsum[wid] = incl;
+    __syncthreads();
+    unsigned wbase = 0;
+    for (int w = 0; w < wid; ++w) wbase += s_wsum[w];
+    unsigned run = wbase + incl - acc;
+#pragma unroll
+    for (int q = 0; q < kBinsPerThread; ++q) {
+      const int p = tid * kBinsPerThread + q;
+      if (p < P) toff[p] = run;
+      run += v[q];
+    }
+    unsigned tile_valid = 0;
+    for (int w = 0; w < kPartThreads / 32; ++w) tile_valid += s_wsum[w];
+    __syncthreads();
+    // 3. counting-sort the tile into shared memory (payloads straight to their sorted slot)
+#pragma unroll
+    for (int j = 0; j < kTileRowsPerThread; ++j) {
+      if (pr[j] < 0) continue;
+      const unsigned slot = toff[pr[j]] + rank[j];
+      skey[slot] = kk[j];
+      srid[slot] = (int32_t)(t0 + j * kPartThreads + tid);
+      spart[slot] = (uint16_t)pr[j];
+#pragma unroll
+      for (int c = 0; c < NP; ++c) reinterpret_cast<uint64_t*>(sm + m.pay[c])[slot] = pv[c][j];
+    }
+    __syncthreads();
+    // 4. loads of the next tile go out before this tile's write-out
+    if (t0 + kTile < hi) fast_load_tile<K, NP>(s, t0 + kTile, hi, kk, pv, live);
+    for (unsigned slot = tid; slot < tile_valid; slot += kPartThreads) {
+      const int p = spart[slot];
+      const int64_t pos = (int64_t)cur[p] + (slot - toff[p]);
+      okeys[pos] = skey[slot];
+      d.rid[pos] = srid[slot];
+#pragma unroll
+      for (int c = 0; c < NP; ++c) {
+        const uint64_t x = reinterpret_cast<const uint64_t*>(sm + m.pay[c])[slot];
+        if (s.pay[c].width == 8) static_cast<unsigned long long*>(d.pay[c])[pos] = x;
+        else static_cast<unsigned int*>(d.pay[c])[pos] = (unsigned int)x;
+      }
+    }
+    __syncthreads();
+    for (int p = tid; p < P; p += kPartThreads) cur[p] += tcnt[p];
+    __syncthreads();
+  }
+}
+
+template <typename K>
+static sj_status launch_fast_scatter(const PartSrc& src, int pbits, int64_t chunk, const int64_t* offs,
+                                     const PartDst& dst, int G, cudaStream_t s) {
+  const FastSmem m = fast_smem(pbits, sizeof(K), src.n_pay);
+  auto go = [&](auto kernel) -> sj_status {
+    SJ_CUDA_TRY(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)m.total));
+    KernelTimer timer("partition_scatter", s);
+    kernel<<<G, kPartThreads, m.total, s>>>(src, pbits, chunk, offs, dst, m);
+    return SJ_OK;
+  };
+  if (src.n_pay == 0) return go(part_scatter_fast_kernel<K, 0>);
+  if (src.n_pay == 1) return go(part_scatter_fast_kernel<K, 1>);
+  return go(part_scatter_fast_kernel<K, 2>);
+}
+
+// Upper bound of the partition grid (scratch sizing); the grid used is never larger.
 static int part_grid(int device) { return sm_count(device) * 4; }
+
+static int scatter_per_sm(const PartSrc& src, int key_type, int pbits, bool fast) {
+  int r = 0;
+  if (fast) {
+    const FastSmem m = fast_smem(pbits, key_type == SJ_INT32 ? 4 : 8, src.n_pay);
+    const void* k = nullptr;
+    if (key_type == SJ_INT32)
+      k = src.n_pay == 0 ? (const void*)part_scatter_fast_kernel<int32_t, 0>
+          : src.n_pay == 1 ? (const void*)part_scatter_fast_kernel<int32_t, 1>
+                           : (const void*)part_scatter_fast_kernel<int32_t, 2>;
+    else
+      k = src.n_pay == 0 ? (const void*)part_scatter_fast_kernel<int64_t, 0>
+          : src.n_pay == 1 ? (const void*)part_scatter_fast_kernel<int64_t, 1>
+                           : (const void*)part_scatter_fast_kernel<int64_t, 2>;
+    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)m.total);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&r, k, kPartThreads, m.total);
+  } else {
+    const ScatterSmem m = scatter_smem(pbits, key_type == SJ_INT32 ? 4 : 8, src);
+    const void* k = key_type == SJ_INT32 ? (const void*)part_scatter_kernel<int32_t>
+                                         : (const void*)part_scatter_kernel<int64_t>;
+    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)m.total);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&r, k, kPartThreads, m.total);
+  }
+  cudaGetLastError();
+  return std::max(1, std::min(4, r));
+}
 
 size_t partition_scratch_bytes(int pbits, int device) {
   const size_t PG = ((size_t)1 << pbits) * part_grid(device);
@@ -224,7 +443,10 @@ sj_status radix_partition(const PartSrc& src, int key_type, int pbits, const Par
                           int device, cudaStream_t s, const int64_t** d_total_out, const int64_t** d_offs_out,
                           int* grid_out) {
   if (pbits < 0 || pbits > kMaxPartBits) return set_error(SJ_ERR_INVALID, "partition bits out of range");
-  const int G = part_grid(device);
+  // Every CTA owns one chunk (no grid-stride loop), so the grid must be resident in one wave:
+  // G = SMs x (the scatter kernel's resident CTAs per SM, at most 4).
+  const bool fast = fast_scatter_ok(src, dst);
+  const int G = sm_count(device) * scatter_per_sm(src, key_type, pbits, fast);
   const int P = 1 << pbits;
   const size_t PG = (size_t)P * G;
   char* base = static_cast<char*>(scratch);
@@ -244,6 +466,15 @@ sj_status radix_partition(const PartSrc& src, int key_type, int pbits, const Par
   {
     KernelTimer timer("partition_scan", s);
     device_exclusive_scan<int32_t, int64_t>(hist, offs, nullptr, (int64_t)PG, tmp, s);
+  }
+  if (fast) {
+    SJ_TRY(key_type == SJ_INT32 ? launch_fast_scatter<int32_t>(src, pbits, chunk, offs, dst, G, s)
+                                : launch_fast_scatter<int64_t>(src, pbits, chunk, offs, dst, G, s));
+    SJ_CUDA_TRY(cudaGetLastError());
+    *d_total_out = offs + PG;
+    *d_offs_out = offs;
+    *grid_out = G;
+    return SJ_OK;
   }
   const ScatterSmem m = scatter_smem(pbits, key_type == SJ_INT32 ? 4 : 8, src);
   if (key_type == SJ_INT32) {

@@ -16,6 +16,7 @@
 // before the first store, so each lane keeps 3R-5R independent loads in flight.
 #include <algorithm>
 
+#include "sj_bulk.cuh"
 #include "sj_device.cuh"
 #include "sj_internal.h"
 #include "sj_probe_direct.h"
@@ -57,11 +58,18 @@ __device__ __forceinline__ void load_rec(const void* p, int stride, uint32_t (&w
   }
 }
 
-template <typename K, bool WIDE, int R, bool CTA_AGG>
+// SP / SB >= 0: a compile-time output shape (SP probe payloads, SB attached build fields from the
+// row store, every width 8 bytes); -1: the shape is read from `a` at run time.
+template <typename K, bool WIDE, int R, bool CTA_AGG, int SP = -1, int SB = -1>
 __global__ void __launch_bounds__(kDirectThreads, (R <= 2 ? 4 : 2))
     probe_direct_kernel(TableDev t, const K* __restrict__ keys, const uint32_t* __restrict__ kv, int64_t kvoff,
                         int64_t n_host, const int64_t* d_n, DirectArgs a) {
   using Ops = SlotOps<WIDE>;
+  constexpr bool kFixed = SP >= 0;
+  const int n_pin = kFixed ? SP : a.n_pin;
+  const int n_bin = kFixed ? SB : a.n_bin;
+  const bool use_rec = kFixed ? SB > 0 : a.rec != nullptr;
+  const int rec_stride = kFixed ? (SB == 1 ? 16 : 32) : a.rec_stride;
   __shared__ unsigned s_wtot[kDirectWarps];
   __shared__ unsigned long long s_wbase[kDirectWarps];
   const int lane = threadIdx.x & 31;
@@ -71,11 +79,15 @@ __global__ void __launch_bounds__(kDirectThreads, (R <= 2 ? 4 : 2))
   constexpr int64_t kRowsCta = (int64_t)kDirectThreads * R;
   const int64_t tiles = (n + kRowsCta - 1) / kRowsCta;
   const uint64_t kmask = ~((1ull << t.rbits) - 1);
-  for (int64_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
-    const int64_t r0 = tile * kRowsCta + (int64_t)warp * (32 * R) + lane;  // row of group j: r0 + 32 j
-    K k[R];
+  const int64_t lane_off = (int64_t)warp * (32 * R) + lane;  // row of group j: tile start + lane_off + 32 j
+  K k[R];
 #pragma unroll
-    for (int j = 0; j < R; ++j) k[j] = r0 + 32 * j < n ? __ldcs(keys + r0 + 32 * j) : (K)0;
+  for (int j = 0; j < R; ++j) {
+    const int64_t r = (int64_t)blockIdx.x * kRowsCta + lane_off + 32 * j;
+    k[j] = r < n ? __ldcs(keys + r) : (K)0;
+  }
+  for (int64_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+    const int64_t r0 = tile * kRowsCta + lane_off;
     uint32_t act = 0;
 #pragma unroll
     for (int j = 0; j < R; ++j) {
@@ -89,6 +101,12 @@ __global__ void __launch_bounds__(kDirectThreads, (R <= 2 ? 4 : 2))
       const uint64_t kb = key_u64<K>(k[j]);
       b[j] = home_bucket(t, kb);
       ks[j] = Ops::probe_key((uint64_t)(long long)k[j] - (uint64_t)t.kmin, kb, t.rbits);
+    }
+    // the next tile's keys load while this tile probes, gathers and writes
+#pragma unroll
+    for (int j = 0; j < R; ++j) {
+      const int64_t r = r0 + (int64_t)gridDim.x * kRowsCta + 32 * j;
+      k[j] = r < n ? __ldcs(keys + r) : (K)0;
     }
     int32_t pos[R];
     uint32_t hit = 0;
@@ -114,6 +132,44 @@ __global__ void __launch_bounds__(kDirectThreads, (R <= 2 ? 4 : 2))
         }
         if (done) act &= ~(1u << j);
         else b[j] = next_bucket(b[j], t.segmask);
+      }
+    }
+    // ---- gather loads for every hit (they need no output position, so they are in flight
+    //      while the output range is reserved) ----
+    int32_t prid[R], brid[R];
+    uint64_t pv[kDirectMaxProbePayload][R];
+    uint64_t bv[kDirectMaxBuildPayload][R];
+#pragma unroll
+    for (int j = 0; j < R; ++j) {
+      prid[j] = brid[j] = 0;
+#pragma unroll
+      for (int c = 0; c < kDirectMaxProbePayload; ++c) pv[c][j] = 0;
+#pragma unroll
+      for (int c = 0; c < kDirectMaxBuildPayload; ++c) bv[c][j] = 0;
+      if (!(hit >> j & 1u)) continue;
+      const int64_t r = r0 + 32 * j;
+      if (a.out_prid) prid[j] = a.prid_map ? __ldcs(a.prid_map + r) : (int32_t)r;
+#pragma unroll
+      for (int c = 0; c < kDirectMaxProbePayload; ++c)
+        if (c < n_pin) pv[c][j] = ld_cs_w(a.pin[c], r, kFixed ? 8 : a.pin_w[c]);
+      if (use_rec) {
+        uint32_t w[8];
+        load_rec(static_cast<const char*>(a.rec) + (int64_t)pos[j] * rec_stride, rec_stride, w);
+        brid[j] = (int32_t)w[0];
+#pragma unroll
+        for (int c = 0; c < kDirectMaxBuildPayload; ++c)
+          bv[c][j] = ((uint64_t)w[3 + 2 * c] << 32) | w[2 + 2 * c];
+      } else {
+        brid[j] = a.brid_map ? __ldg(reinterpret_cast<const int32_t*>(reinterpret_cast<const char*>(a.brid_map) +
+                                                                       (int64_t)pos[j] * a.brid_stride))
+                             : pos[j];
+#pragma unroll
+        for (int c = 0; c < kDirectMaxBuildPayload; ++c) {
+          if (c < n_bin) {
+            const int64_t i = a.bin_by_pos ? pos[j] : brid[j];
+            bv[c][j] = ld_nc_w(static_cast<const char*>(a.bin[c]) + i * a.bin_stride[c], a.bin_w[c]);
+          }
+        }
       }
     }
     unsigned bal[R];
@@ -149,8 +205,6 @@ __global__ void __launch_bounds__(kDirectThreads, (R <= 2 ? 4 : 2))
       base = __shfl_sync(kFullMask, base, 0);
     }
     if (wtot == 0) continue;
-
-    // ---- gather loads for every hit of the tile ----
     int64_t p[R];
     {
       unsigned run = 0;
@@ -160,29 +214,170 @@ __global__ void __launch_bounds__(kDirectThreads, (R <= 2 ? 4 : 2))
         run += __popc(bal[j]);
       }
     }
-    int32_t prid[R], brid[R];
-    uint64_t pv[kDirectMaxProbePayload][R];
+    // ---- stores: each row group j is one contiguous run of positions per column ----
+#pragma unroll
+    for (int j = 0; j < R; ++j) {
+      if (!(hit >> j & 1u) || p[j] >= a.capacity) continue;
+      if (a.out_prid) __stcs(a.out_prid + p[j], prid[j]);
+      if (a.out_brid) __stcs(a.out_brid + p[j], brid[j]);
+#pragma unroll
+      for (int c = 0; c < kDirectMaxProbePayload; ++c)
+        if (c < n_pin) st_cs_w(a.pout[c], p[j], kFixed ? 8 : a.pin_w[c], pv[c][j]);
+#pragma unroll
+      for (int c = 0; c < kDirectMaxBuildPayload; ++c)
+        if (c < n_bin) st_cs_w(a.bout[c], p[j], kFixed ? 8 : a.bin_w[c], bv[c][j]);
+    }
+  }
+}
+
+// ------------------------------------------------------------------------------------------------
+// The same probe with its streaming inputs staged by the TMA engine. The probe rows of a tile
+// (keys, partition row ids, probe payloads: contiguous ranges) are bulk-copied into a 3-stage
+// shared-memory ring two tiles ahead of their use, so no lane waits on DRAM for them and no
+// register holds them in flight; the lanes only wait on the table (bucket, then record) in L2.
+// Stage of iteration i: i % 3; tile i+2 is issued right after iteration i's first CTA barrier,
+// which every reader of that stage (iteration i-1) has passed. Only full tiles are staged; the
+// last, partial tile of the probe reads global memory directly. A bounded mbarrier wait that runs
+// out makes the whole CTA stop after its next barrier and marks the count negative (bit 63).
+// ------------------------------------------------------------------------------------------------
+constexpr int kTmaR = 2;
+constexpr int kTmaTile = kDirectThreads * kTmaR;
+constexpr int kTmaStages = 3;
+
+struct TmaStage {
+  int32_t key_off, rid_off, pay_off[kDirectMaxProbePayload], bytes;  // within a stage
+};
+
+template <typename K>
+__host__ __device__ inline TmaStage tma_stage(const DirectArgs& a) {
+  TmaStage st{};
+  int o = 0;
+  st.key_off = o;
+  o += kTmaTile * (int)sizeof(K);
+  st.rid_off = o;
+  if (a.prid_map) o += kTmaTile * 4;
+  for (int c = 0; c < kDirectMaxProbePayload; ++c) {
+    st.pay_off[c] = o;
+    if (c < a.n_pin) o += kTmaTile * a.pin_w[c];
+  }
+  st.bytes = (o + 127) & ~127;
+  return st;
+}
+
+template <typename K, bool WIDE>
+__global__ void __launch_bounds__(kDirectThreads, 4)
+    probe_tma_kernel(TableDev t, const K* __restrict__ keys, const uint32_t* __restrict__ kv, int64_t kvoff,
+                     int64_t n_host, const int64_t* d_n, DirectArgs a, TmaStage st) {
+  using Ops = SlotOps<WIDE>;
+  constexpr int R = kTmaR;
+  extern __shared__ __align__(128) unsigned char s_ring[];
+  __shared__ __align__(8) uint64_t s_bar[kTmaStages];
+  __shared__ unsigned s_wtot[kDirectWarps];
+  __shared__ unsigned long long s_wbase[kDirectWarps];
+  __shared__ int s_abort;
+  const int lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
+  const unsigned below = (1u << lane) - 1u;
+  const int64_t n = d_n ? *d_n : n_host;
+  const int64_t tiles = (n + kTmaTile - 1) / kTmaTile;
+  const int64_t full_tiles = n / kTmaTile;
+  const uint64_t kmask = ~((1ull << t.rbits) - 1);
+  const int li = warp * (32 * R) + lane;  // row of group j inside a tile: li + 32 j
+
+  auto issue = [&](int64_t tt, int sidx) {  // thread 0; tt < full_tiles
+    unsigned char* sb = s_ring + sidx * st.bytes;
+    uint32_t bytes = kTmaTile * (uint32_t)sizeof(K);
+    if (a.prid_map) bytes += kTmaTile * 4;
+    for (int c = 0; c < a.n_pin; ++c) bytes += kTmaTile * a.pin_w[c];
+    mbar_arrive_expect_tx(&s_bar[sidx], bytes);
+    bulk_copy_g2s(sb + st.key_off, keys + tt * kTmaTile, kTmaTile * sizeof(K), &s_bar[sidx]);
+    if (a.prid_map) bulk_copy_g2s(sb + st.rid_off, a.prid_map + tt * kTmaTile, kTmaTile * 4, &s_bar[sidx]);
+    for (int c = 0; c < a.n_pin; ++c)
+      bulk_copy_g2s(sb + st.pay_off[c], static_cast<const char*>(a.pin[c]) + tt * kTmaTile * a.pin_w[c],
+                    kTmaTile * a.pin_w[c], &s_bar[sidx]);
+  };
+
+  if (threadIdx.x == 0) {
+    for (int q = 0; q < kTmaStages; ++q) mbar_init(&s_bar[q], 1);
+    mbar_init_fence();
+    s_abort = 0;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    if (blockIdx.x < full_tiles) issue(blockIdx.x, 0);
+    if (blockIdx.x + gridDim.x < full_tiles) issue(blockIdx.x + gridDim.x, 1);
+  }
+  int it = 0;
+  for (int64_t tile = blockIdx.x; tile < tiles; tile += gridDim.x, ++it) {
+    const int sidx = it % kTmaStages;
+    const unsigned char* sb = s_ring + sidx * st.bytes;
+    const bool staged = tile < full_tiles;
+    const int64_t r0 = tile * kTmaTile + li;
+    bool ok = true;
+    if (staged) ok = mbar_wait_bounded(&s_bar[sidx], (uint32_t)((it / kTmaStages) & 1), kBulkWaitPolls);
+    K k[R];
+#pragma unroll
+    for (int j = 0; j < R; ++j) {
+      const int64_t r = r0 + 32 * j;
+      if (staged) k[j] = reinterpret_cast<const K*>(sb + st.key_off)[li + 32 * j];
+      else k[j] = r < n ? __ldcs(keys + r) : (K)0;
+    }
+    uint32_t act = 0;
+#pragma unroll
+    for (int j = 0; j < R; ++j) {
+      const int64_t r = r0 + 32 * j;
+      if (ok && r < n && bit_valid(kv, kvoff, r) && in_range(t, k[j])) act |= 1u << j;
+    }
+    if (!ok) s_abort = 1;
+    uint32_t b[R];
+    uint64_t ks[R];
+#pragma unroll
+    for (int j = 0; j < R; ++j) {
+      const uint64_t kb = key_u64<K>(k[j]);
+      b[j] = home_bucket(t, kb);
+      ks[j] = Ops::probe_key((uint64_t)(long long)k[j] - (uint64_t)t.kmin, kb, t.rbits);
+    }
+    int32_t pos[R];
+    uint32_t hit = 0;
+#pragma unroll
+    for (int j = 0; j < R; ++j) pos[j] = 0;
+    for (uint32_t step = 0; act && step <= t.segmask; ++step) {
+      Bucket bk[R];
+#pragma unroll
+      for (int j = 0; j < R; ++j)
+        if (act >> j & 1u) bk[j] = load_bucket<true>(t.slots, b[j]);
+#pragma unroll
+      for (int j = 0; j < R; ++j) {
+        if (!(act >> j & 1u)) continue;
+        bool done = false;
+#pragma unroll
+        for (int q = 0; q < Ops::kSlots; ++q) {
+          if (!done && Ops::match_s(bk[j], q, ks[j], kmask)) {
+            pos[j] = Ops::rid(bk[j], q, t.rbits);
+            hit |= 1u << j;
+            done = true;
+          }
+          done |= Ops::empty(bk[j], q);
+        }
+        if (done) act &= ~(1u << j);
+        else b[j] = next_bucket(b[j], t.segmask);
+      }
+    }
+    // build-side gather loads (the probe-side values stay in the stage until the stores)
+    int32_t brid[R];
     uint64_t bv[kDirectMaxBuildPayload][R];
 #pragma unroll
     for (int j = 0; j < R; ++j) {
-      prid[j] = brid[j] = 0;
-#pragma unroll
-      for (int c = 0; c < kDirectMaxProbePayload; ++c) pv[c][j] = 0;
+      brid[j] = 0;
 #pragma unroll
       for (int c = 0; c < kDirectMaxBuildPayload; ++c) bv[c][j] = 0;
       if (!(hit >> j & 1u)) continue;
-      const int64_t r = r0 + 32 * j;
-      if (a.out_prid) prid[j] = a.prid_map ? __ldcs(a.prid_map + r) : (int32_t)r;
-#pragma unroll
-      for (int c = 0; c < kDirectMaxProbePayload; ++c)
-        if (c < a.n_pin) pv[c][j] = ld_cs_w(a.pin[c], r, a.pin_w[c]);
       if (a.rec) {
         uint32_t w[8];
         load_rec(static_cast<const char*>(a.rec) + (int64_t)pos[j] * a.rec_stride, a.rec_stride, w);
         brid[j] = (int32_t)w[0];
 #pragma unroll
-        for (int c = 0; c < kDirectMaxBuildPayload; ++c)
-          bv[c][j] = ((uint64_t)w[3 + 2 * c] << 32) | w[2 + 2 * c];
+        for (int c = 0; c < kDirectMaxBuildPayload; ++c) bv[c][j] = ((uint64_t)w[3 + 2 * c] << 32) | w[2 + 2 * c];
       } else {
         brid[j] = a.brid_map ? __ldg(reinterpret_cast<const int32_t*>(reinterpret_cast<const char*>(a.brid_map) +
                                                                        (int64_t)pos[j] * a.brid_stride))
@@ -196,19 +391,73 @@ __global__ void __launch_bounds__(kDirectThreads, (R <= 2 ? 4 : 2))
         }
       }
     }
-    // ---- stores: each row group j is one contiguous run of positions per column ----
+    unsigned bal[R];
+    unsigned wtot = 0;
 #pragma unroll
     for (int j = 0; j < R; ++j) {
-      if (!(hit >> j & 1u) || p[j] >= a.capacity) continue;
-      if (a.out_prid) __stcs(a.out_prid + p[j], prid[j]);
-      if (a.out_brid) __stcs(a.out_brid + p[j], brid[j]);
+      bal[j] = __ballot_sync(kFullMask, (hit >> j) & 1u);
+      wtot += __popc(bal[j]);
+    }
+    // CTA reservation; the first barrier also frees stage (it + 2) % 3 for tile it + 2
+    if (lane == 0) s_wtot[warp] = wtot;
+    __syncthreads();
+    if (s_abort) break;
+    if (threadIdx.x == 0) {
+      const int64_t t2 = tile + 2 * (int64_t)gridDim.x;
+      if (t2 < full_tiles) issue(t2, (it + 2) % kTmaStages);
+    }
+    if (warp == 0) {
+      const unsigned v = lane < kDirectWarps ? s_wtot[lane] : 0u;
+      unsigned incl = v;
 #pragma unroll
-      for (int c = 0; c < kDirectMaxProbePayload; ++c)
-        if (c < a.n_pin) st_cs_w(a.pout[c], p[j], a.pin_w[c], pv[c][j]);
+      for (int d = 1; d < kDirectWarps; d <<= 1) {
+        const unsigned o = __shfl_up_sync(kFullMask, incl, d);
+        if (lane >= d) incl += o;
+      }
+      const unsigned tot = __shfl_sync(kFullMask, incl, kDirectWarps - 1);
+      unsigned long long cb = 0;
+      if (lane == 0 && tot) cb = atomicAdd(a.d_count, (unsigned long long)tot);
+      cb = __shfl_sync(kFullMask, cb, 0);
+      if (lane < kDirectWarps) s_wbase[lane] = cb + (incl - v);
+    }
+    __syncthreads();
+    if (wtot == 0) continue;
+    const unsigned long long base = s_wbase[warp];
+    unsigned run = 0;
+#pragma unroll
+    for (int j = 0; j < R; ++j) {
+      const int64_t p = (int64_t)(base + run + __popc(bal[j] & below));
+      run += __popc(bal[j]);
+      if (!(hit >> j & 1u) || p >= a.capacity) continue;
+      const int64_t r = r0 + 32 * j;
+      const int i = li + 32 * j;
+      if (a.out_prid) {
+        int32_t pr;
+        if (!a.prid_map) pr = (int32_t)r;
+        else if (staged) pr = reinterpret_cast<const int32_t*>(sb + st.rid_off)[i];
+        else pr = __ldcs(a.prid_map + r);
+        __stcs(a.out_prid + p, pr);
+      }
+      if (a.out_brid) __stcs(a.out_brid + p, brid[j]);
+#pragma unroll
+      for (int c = 0; c < kDirectMaxProbePayload; ++c) {
+        if (c < a.n_pin) {
+          uint64_t v;
+          if (staged) v = a.pin_w[c] == 8 ? reinterpret_cast<const uint64_t*>(sb + st.pay_off[c])[i]
+                                          : reinterpret_cast<const uint32_t*>(sb + st.pay_off[c])[i];
+          else v = ld_cs_w(a.pin[c], r, a.pin_w[c]);
+          st_cs_w(a.pout[c], p, a.pin_w[c], v);
+        }
+      }
 #pragma unroll
       for (int c = 0; c < kDirectMaxBuildPayload; ++c)
-        if (c < a.n_bin) st_cs_w(a.bout[c], p[j], a.bin_w[c], bv[c][j]);
+        if (c < a.n_bin) st_cs_w(a.bout[c], p, a.bin_w[c], bv[c][j]);
     }
+  }
+  if (s_abort && threadIdx.x == 0) {
+    atomicOr(a.d_count, 1ull << 63);
+    // let copies still in flight land before the CTA's shared memory is released
+    for (int q = 0; q < kTmaStages; ++q) mbar_wait_bounded(&s_bar[q], 0, 64);
   }
 }
 
@@ -258,20 +507,40 @@ bool direct_args(const GatherArgs& g, DirectArgs& a) {
   return true;
 }
 
+// The compile-time shape (SP, SB) that `a` has, or (-1, -1).
+static void fixed_shape(const DirectArgs& a, int& sp, int& sb) {
+  sp = sb = -1;
+  for (int c = 0; c < a.n_pin; ++c)
+    if (a.pin_w[c] != 8) return;
+  if (a.n_bin > 0 && (!a.rec || a.rec_stride != (a.n_bin == 1 ? 16 : 32))) return;
+  if (a.n_bin == 0 && a.rec) return;
+  sp = a.n_pin;
+  sb = a.n_bin;
+}
+
+template <typename K, bool WIDE, int R, bool CTA, int SP, int SB>
+static void launch_direct_shape(const sj_table* t, const sj_column& p, const int64_t* d_n, const DirectArgs& a,
+                                cudaStream_t s) {
+  int resident = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, probe_direct_kernel<K, WIDE, R, CTA, SP, SB>,
+                                                kDirectThreads, 0);
+  const int64_t tiles = (p.num_rows + (int64_t)kDirectThreads * R - 1) / ((int64_t)kDirectThreads * R);
+  const int per_sm = std::min(std::max(1, resident), std::max(1, t->params.ctas_per_sm));
+  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(tiles, (int64_t)sm_count(t->device) * per_sm));
+  probe_direct_kernel<K, WIDE, R, CTA, SP, SB><<<grid, kDirectThreads, 0, s>>>(
+      table_dev(t), static_cast<const K*>(p.data), p.validity, p.validity_offset, p.num_rows, d_n, a);
+}
+
 template <typename K, bool WIDE, int R, bool CTA>
 static void launch_direct_kernel(const sj_table* t, const sj_column& p, const int64_t* d_n, const DirectArgs& a,
                                  cudaStream_t s) {
-  static int resident = 0;  // CTAs per SM of this instantiation (same on every B200)
-  if (resident == 0) {
-    int r = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&r, probe_direct_kernel<K, WIDE, R, CTA>, kDirectThreads, 0);
-    resident = std::max(1, r);
-  }
-  const int64_t tiles = (p.num_rows + (int64_t)kDirectThreads * R - 1) / ((int64_t)kDirectThreads * R);
-  const int per_sm = std::min(resident, std::max(1, t->params.ctas_per_sm));
-  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(tiles, (int64_t)sm_count(t->device) * per_sm));
-  probe_direct_kernel<K, WIDE, R, CTA><<<grid, kDirectThreads, 0, s>>>(
-      table_dev(t), static_cast<const K*>(p.data), p.validity, p.validity_offset, p.num_rows, d_n, a);
+  int sp, sb;
+  fixed_shape(a, sp, sb);
+  // the shapes of the large foreign-key join (1 probe, 2 build payloads) and of a served lookup
+  // (1 build payload) get compile-time specialisations when 2 rows per lane are used
+  if (R == 2 && sp == 1 && sb == 2) return launch_direct_shape<K, WIDE, R, CTA, 1, 2>(t, p, d_n, a, s);
+  if (R == 2 && sp == 0 && sb == 1) return launch_direct_shape<K, WIDE, R, CTA, 0, 1>(t, p, d_n, a, s);
+  launch_direct_shape<K, WIDE, R, CTA, -1, -1>(t, p, d_n, a, s);
 }
 
 template <typename K, bool WIDE>
@@ -286,11 +555,46 @@ static void launch_direct(const sj_table* t, const sj_column& p, const int64_t* 
   }
 }
 
+static bool al16(const void* p) { return ((uintptr_t)p & 15u) == 0; }
+
+template <typename K, bool WIDE>
+static void launch_tma(const sj_table* t, const sj_column& p, const int64_t* d_n, const DirectArgs& a,
+                       cudaStream_t s) {
+  const TmaStage st = tma_stage<K>(a);
+  const size_t smem = (size_t)kTmaStages * st.bytes;
+  if (smem > 48 * 1024)
+    cudaFuncSetAttribute(probe_tma_kernel<K, WIDE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  int resident = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, probe_tma_kernel<K, WIDE>, kDirectThreads, smem);
+  const int64_t tiles = (p.num_rows + kTmaTile - 1) / kTmaTile;
+  const int per_sm = std::min(std::max(1, resident), std::max(1, t->params.ctas_per_sm));
+  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(tiles, (int64_t)sm_count(t->device) * per_sm));
+  probe_tma_kernel<K, WIDE><<<grid, kDirectThreads, smem, s>>>(
+      table_dev(t), static_cast<const K*>(p.data), p.validity, p.validity_offset, p.num_rows, d_n, a, st);
+}
+
 bool probe_direct(const sj_table* t, const sj_column& p, const int64_t* d_n, const GatherArgs& g, cudaStream_t s) {
   const sj_join_params& pr = t->params;
   if (pr.probe_kernel == SJ_PROBE_KERNEL_STAGED) return false;
   DirectArgs a;
   if (!direct_args(g, a)) return false;
+  // AUTO takes the plain-load kernel: on the large 1:1 join the TMA ring's per-tile CTA barriers
+  // cost more than the DRAM latency it hides (measured 1.96 vs 1.73 ms per 64M probe rows)
+  bool tma = pr.probe_kernel == SJ_PROBE_KERNEL_DIRECT_TMA;
+  tma = tma && al16(p.data) && (!a.prid_map || al16(a.prid_map));
+  for (int c = 0; c < a.n_pin; ++c) tma = tma && al16(a.pin[c]);
+  if (tma) {
+    KernelTimer timer("probe_direct", s);
+    const bool wide = t->slot_kind == SJ_SLOT_WIDE128;
+    if (t->key_type == SJ_INT32) {
+      if (wide) launch_tma<int32_t, true>(t, p, d_n, a, s);
+      else launch_tma<int32_t, false>(t, p, d_n, a, s);
+    } else {
+      if (wide) launch_tma<int64_t, true>(t, p, d_n, a, s);
+      else launch_tma<int64_t, false>(t, p, d_n, a, s);
+    }
+    return true;
+  }
   const int agg = pr.aggregation;
   const bool cta = agg == SJ_AGG_CTA || (agg == SJ_AGG_AUTO && p.num_rows >= (1 << 20));
   const int rpl = pr.rows_per_lane > 0 ? pr.rows_per_lane : 2;

@@ -694,7 +694,7 @@ static sj_status probe_partitioned(const sj_table* t, const sj_column& p, Gather
   const int64_t n = p.num_rows;
   const int pbits = probe_partition_bits(t);
   const int kw = t->key_type == SJ_INT32 ? 4 : 8;
-  size_t bytes = align256((size_t)n * kw) + align256((size_t)n * 4) + partition_scratch_bytes(pbits, t->device);
+  size_t bytes = align256((size_t)n * kw) + align256((size_t)n * 4) + partition_scratch_bytes(pbits, t->device) + 256;
   for (int c = 0; c < g.n_pin; ++c)
     bytes += align256((size_t)n * g.pin[c].width) + (g.pin[c].valid ? align256((size_t)n) : 0);
   Scratch sc;
@@ -720,6 +720,7 @@ static sj_status probe_partitioned(const sj_table* t, const sj_column& p, Gather
     pd.valid8[c] = g.pin[c].valid ? reinterpret_cast<uint8_t*>(carve((size_t)n)) : nullptr;
   }
   void* pscratch = carve(partition_scratch_bytes(pbits, t->device));
+  unsigned long long* tile_ctr = reinterpret_cast<unsigned long long*>(carve(8));
   const int64_t *d_total, *d_offs;
   int G;
   SJ_TRY(radix_partition(ps, t->key_type, pbits, pd, pscratch, t->device, s, &d_total, &d_offs, &G));
@@ -727,7 +728,7 @@ static sj_status probe_partitioned(const sj_table* t, const sj_column& p, Gather
   for (int c = 0; c < g.n_pin; ++c)
     g.pin[c] = PayloadIn{pd.pay[c], nullptr, pd.valid8[c], 0, g.pin[c].width, g.pin[c].width, 1, 0};
   const sj_column pk{pd.keys, nullptr, 0, n, t->key_type, 0};
-  if (!probe_direct(t, pk, d_total, g, s)) dispatch_distinct<false>(t, pk, d_total, g, s);
+  if (!probe_direct(t, pk, d_total, g, s, tile_ctr)) dispatch_distinct<false>(t, pk, d_total, g, s);
   SJ_CUDA_TRY(cudaGetLastError());
   return SJ_OK;
 }
@@ -750,7 +751,9 @@ sj_status probe_gather(const sj_table* t, const sj_column& p, const GatherSpec& 
 
   if (t->layout == SJ_LAYOUT_DISTINCT) {
     if (t->pbits > 0 && p.num_rows >= kMinPartitionedProbe) return probe_partitioned(t, p, g, alloc, s);
-    if (!probe_direct(t, p, nullptr, g, s)) dispatch_distinct<false>(t, p, nullptr, g, s);
+    Scratch ctr;
+    SJ_TRY(ctr.get(alloc, 256, s));
+    if (!probe_direct(t, p, nullptr, g, s, ctr.as<unsigned long long>())) dispatch_distinct<false>(t, p, nullptr, g, s);
     SJ_CUDA_TRY(cudaGetLastError());
     return SJ_OK;
   }

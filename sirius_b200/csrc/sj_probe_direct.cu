@@ -80,13 +80,18 @@ __global__ void __launch_bounds__(kDirectThreads, (R <= 2 ? 4 : 2))
   const int64_t tiles = (n + kRowsCta - 1) / kRowsCta;
   const uint64_t kmask = ~((1ull << t.rbits) - 1);
   const int64_t lane_off = (int64_t)warp * (32 * R) + lane;  // row of group j: tile start + lane_off + 32 j
+  __shared__ int64_t s_next;
   K k[R];
 #pragma unroll
   for (int j = 0; j < R; ++j) {
     const int64_t r = (int64_t)blockIdx.x * kRowsCta + lane_off + 32 * j;
     k[j] = r < n ? __ldcs(keys + r) : (K)0;
   }
-  for (int64_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+  // Tiles: the first two of a CTA are static (blockIdx.x, + gridDim.x); with CTA reservation the
+  // later ones come from a shared tile counter, so the CTAs sweep the (partition-ordered) probe
+  // rows together and the table rows in use stay one partition's worth, resident in L2.
+  int64_t tile = blockIdx.x, nxt = tile + gridDim.x;
+  while (tile < tiles) {
     const int64_t r0 = tile * kRowsCta + lane_off;
     uint32_t act = 0;
 #pragma unroll
@@ -105,7 +110,7 @@ __global__ void __launch_bounds__(kDirectThreads, (R <= 2 ? 4 : 2))
     // the next tile's keys load while this tile probes, gathers and writes
 #pragma unroll
     for (int j = 0; j < R; ++j) {
-      const int64_t r = r0 + (int64_t)gridDim.x * kRowsCta + 32 * j;
+      const int64_t r = nxt * kRowsCta + lane_off + 32 * j;
       k[j] = r < n ? __ldcs(keys + r) : (K)0;
     }
     int32_t pos[R];
@@ -194,6 +199,7 @@ __global__ void __launch_bounds__(kDirectThreads, (R <= 2 ? 4 : 2))
         const unsigned tot = __shfl_sync(kFullMask, incl, kDirectWarps - 1);
         unsigned long long cb = 0;
         if (lane == 0 && tot) cb = atomicAdd(a.d_count, (unsigned long long)tot);
+        if (lane == 1) s_next = 2 * (int64_t)gridDim.x + (int64_t)atomicAdd(a.tile_ctr, 1ull);
         cb = __shfl_sync(kFullMask, cb, 0);
         if (lane < kDirectWarps) s_wbase[lane] = cb + (incl - v);
       }
@@ -204,6 +210,8 @@ __global__ void __launch_bounds__(kDirectThreads, (R <= 2 ? 4 : 2))
       if (lane == 0 && wtot) base = atomicAdd(a.d_count, (unsigned long long)wtot);
       base = __shfl_sync(kFullMask, base, 0);
     }
+    tile = nxt;
+    nxt = CTA_AGG ? s_next : nxt + gridDim.x;
     if (wtot == 0) continue;
     int64_t p[R];
     {
@@ -573,11 +581,14 @@ static void launch_tma(const sj_table* t, const sj_column& p, const int64_t* d_n
       table_dev(t), static_cast<const K*>(p.data), p.validity, p.validity_offset, p.num_rows, d_n, a, st);
 }
 
-bool probe_direct(const sj_table* t, const sj_column& p, const int64_t* d_n, const GatherArgs& g, cudaStream_t s) {
+bool probe_direct(const sj_table* t, const sj_column& p, const int64_t* d_n, const GatherArgs& g, cudaStream_t s,
+                  unsigned long long* tile_ctr) {
   const sj_join_params& pr = t->params;
   if (pr.probe_kernel == SJ_PROBE_KERNEL_STAGED) return false;
   DirectArgs a;
   if (!direct_args(g, a)) return false;
+  if (cudaMemsetAsync(tile_ctr, 0, sizeof(unsigned long long), s) != cudaSuccess) return false;
+  a.tile_ctr = tile_ctr;
   // AUTO takes the plain-load kernel: on the large 1:1 join the TMA ring's per-tile CTA barriers
   // cost more than the DRAM latency it hides (measured 1.96 vs 1.73 ms per 64M probe rows)
   bool tma = pr.probe_kernel == SJ_PROBE_KERNEL_DIRECT_TMA;

@@ -28,6 +28,7 @@ struct DirectArgs {
   void* bout[kDirectMaxBuildPayload];
   int64_t capacity;
   unsigned long long* d_count;
+  unsigned long long* tile_ctr;  // zeroed device word: dynamic tile order of CTA-reserving launches
 };
 
 // Fills `a` from a general gather description; false when the output shape needs the staged
@@ -36,6 +37,8 @@ bool direct_args(const GatherArgs& g, DirectArgs& a);
 
 // Launches the direct probe of DISTINCT table `t` when the shape allows and the table's
 // parameters do not ask for the staged kernel; returns false (nothing launched) otherwise.
-bool probe_direct(const sj_table* t, const sj_column& p, const int64_t* d_n, const GatherArgs& g, cudaStream_t s);
+// `tile_ctr`: a device word the launch may use as its tile counter (zeroed here, on `s`).
+bool probe_direct(const sj_table* t, const sj_column& p, const int64_t* d_n, const GatherArgs& g, cudaStream_t s,
+                  unsigned long long* tile_ctr);
 
 }  // namespace sj

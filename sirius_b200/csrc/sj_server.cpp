@@ -122,9 +122,10 @@ static void size_request(const sj_server* S, SrvReq* r) {
   r->out_bytes = out;
   const int kw = T.t->key_type == SJ_INT32 ? 4 : 8;
   // a partitioned probe: partitioned keys + row ids + the partition histogram / offsets
-  r->scratch_bytes = T.t->pbits > 0 && n >= kMinPartitionedProbe
-                         ? a256((size_t)n * kw) + a256((size_t)n * 4) + partition_scratch_bytes(T.t->pbits, S->device)
-                         : 0;
+  r->scratch_bytes = 256 + (T.t->pbits > 0 && n >= kMinPartitionedProbe
+                               ? a256((size_t)n * kw) + a256((size_t)n * 4) +
+                                     partition_scratch_bytes(T.t->pbits, S->device) + 256
+                               : 0);
 }
 
 static void CUDART_CB on_request_done(void* p) {

@@ -59,7 +59,7 @@ def parse():
     ap.add_argument("--probe-kernel", type=int, default=0, help="0 auto, 1 staged write-out, 2 direct write-out")
     ap.add_argument("--rows-per-lane", type=int, default=0)
     ap.add_argument("--ctas-per-sm", type=int, default=0)
-    ap.add_argument("--workload", default="large", choices=["large", "batched", "served"])
+    ap.add_argument("--workload", default="large", choices=["large", "small", "skewed", "batched", "served"])
     ap.add_argument("--autotune", action="store_true", help="batched: choose launch parameters by the autotuner")
     ap.add_argument("--requests", type=int, default=2000)
     ap.add_argument("--slots", type=int, default=4)
@@ -671,6 +671,120 @@ def run_served(args):
     return 0
 
 
+# --------------------------------------------------------------------------------------------
+# small (100K x 1M int32) and skewed (8M Zipf x 32M Zipf + 5% NULL, int64) workloads
+# --------------------------------------------------------------------------------------------
+def run_other(args):
+    """Probe phase of the small or skewed join against a resident table (attached build payload),
+    the same metric as the large workload; correctness spot checks use torch on the device."""
+    import torch
+    from sirius_b200 import datagen as D
+    from sirius_b200 import join as J
+    from sirius_b200 import _lib
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    inp = D.small(args.seed) if args.workload == "small" else D.skewed(args.seed)
+    bk = torch.from_numpy(inp.build_keys).to(dev)
+    pk = torch.from_numpy(inp.probe_keys).to(dev)
+    pv = None if inp.probe_validity is None else torch.from_numpy(inp.probe_validity.view(np.int32)).to(dev)
+    bp = [torch.from_numpy(c).to(dev) for c in inp.build_payload]
+    pp = [torch.from_numpy(c).to(dev) for c in inp.probe_payload]
+    t_build = []
+    for i in range(3):
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        tb = J.HashTable(bk, attach=bp, partition_bits=args.partition_bits)
+        e1.record()
+        torch.cuda.synchronize()
+        t_build.append(e0.elapsed_time(e1))
+        if i < 2:
+            tb.close()
+    info = tb.info()
+    m = int(tb.count(pk, pv).item())
+    # expected output size from the key multiplicities (torch, independent of the join kernels)
+    uk, cnt = torch.unique(bk, return_counts=True)
+    idx = torch.searchsorted(uk, pk).clamp(max=uk.numel() - 1)
+    mult = torch.where(uk[idx] == pk, cnt[idx], torch.zeros_like(cnt[idx]))
+    if pv is not None:
+        valid = ((pv.view(torch.int32).long().repeat_interleave(32)[: pk.numel()] >>
+                  (torch.arange(pk.numel(), device=dev) % 32)) & 1).bool()
+        mult = torch.where(valid, mult, torch.zeros_like(mult))
+    assert m == int(mult.sum().item()), "match count differs from the key multiplicities"
+    out = J.allocate_output(m, pp, bp, dev)
+    d_count = torch.zeros(1, dtype=torch.int64, device=dev)
+
+    def step():
+        tb.probe_gather(pk, pv, pp, attached=True, capacity=m, out=out, d_count=d_count, sync=False)
+
+    for _ in range(max(3, args.warmup)):
+        step()
+    torch.cuda.synchronize()
+    assert int(d_count.item()) == m
+    sample = torch.randint(0, m, (1 << 16,), device=dev)
+    assert torch.equal(pk[out.probe_rid[sample].long()], bk[out.build_rid[sample].long()]), "joined keys differ"
+    _lib.timing_collect()
+    _lib.timing_enable(True)
+    with ClockSampler(0) as clk:
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(args.steps):
+            step()
+        e1.record()
+        torch.cuda.synchronize()
+    _lib.timing_enable(False)
+    kt = _lib.timing_collect()
+    ms = e0.elapsed_time(e1) / args.steps
+    alg = (inp.probe_keys.nbytes + (0 if inp.probe_validity is None else inp.probe_validity.nbytes) +
+           sum(c.nbytes for c in inp.probe_payload) + sum(c.nbytes for c in inp.build_payload) +
+           m * inp.output_row_bytes())
+    peak, peak_src = measured_peak()
+    achieved = alg / (ms / 1e3) / 1e9
+    per_kernel = {}
+    for name, kms in kt:
+        k = per_kernel.setdefault(name, [0, 0.0])
+        k[0] += 1
+        k[1] += kms
+    ktot = sum(v[1] for v in per_kernel.values()) or 1.0
+    kernels = {n: {"launches": c, "ms_per_launch": round(t / c, 4), "share": round(t / ktot, 4)}
+               for n, (c, t) in sorted(per_kernel.items(), key=lambda kv: -kv[1][1])}
+    cpu = None
+    if not args.no_cpu and args.cpu_steps > 0:
+        from oracle import oracle as O
+        O.build()
+        threads = O.default_threads()
+        ts = []
+        for _ in range(args.cpu_steps):
+            t0 = time.perf_counter()
+            r = O.hash_join(inp.build_keys, inp.probe_keys, None, inp.probe_validity, probe_payload=inp.probe_payload,
+                            build_payload=inp.build_payload, threads=threads, capacity=m)
+            ts.append(time.perf_counter() - t0)
+            assert r.rows == m
+        cpu = {"value": round(inp.n_probe / statistics.median(ts) / 1e6, 3), "unit": "Mtuples/s", "cores": threads,
+               "kind": "port", "sample": f"full workload, {len(ts)} one-shot CPU joins, median {statistics.median(ts):.3f} s"}
+    desc = ("small: build 100,000 unique int32 keys (permutation) + int32 payload; probe 1,000,000 int32 keys "
+            "uniform over 0..109,999 + int32 payload" if args.workload == "small" else
+            "skewed: build 8M int64 keys Zipf(1.1) over 1M values + int32 payload; probe 32M int64 keys Zipf(0.8) "
+            "over 2M values (half absent), 5% NULL")
+    line = {
+        "metric": "join probe Mtuples/s", "value": round(inp.n_probe / (ms / 1e3) / 1e6, 3), "unit": "Mtuples/s",
+        "n_gpus": 1, "steps": args.steps, "warmup": max(3, args.warmup), "ms_per_step": round(ms, 4),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "int32" if args.workload == "small" else "int64", "data": "synthetic (seeded numpy)",
+        "config": {"workload": desc, "build_rows": inp.n_build, "probe_rows": inp.n_probe, "matches": m,
+                   "table": {"layout": "DISTINCT" if info.layout == 1 else "GROUPED",
+                             "slot": "PACKED64" if info.slot_kind == 0 else "WIDE128",
+                             "partition_bits": int(info.partition_bits), "max_group": int(info.max_group)},
+                   "t_build_ms": round(min(t_build), 3)},
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 4), "traffic": None, "alg_bytes_per_launch": int(alg),
+                     "launch_ms": round(ms, 4), "kernels": kernels, "peak_source": peak_src},
+        "cpu_baseline": cpu, "gpu_launches": len(kt), "clocks": clk.summary(),
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -679,6 +793,8 @@ def main():
         return run_batched(args)
     if args.workload == "served":
         return run_served(args)
+    if args.workload in ("small", "skewed"):
+        return run_other(args)
     return run_sj(args)
 
 

@@ -232,6 +232,8 @@ SJ_EXPORT sj_status sj_probe_count(const sj_table* table, const sj_column* probe
  * gathers the attached columns (in attach order) instead of caller columns.
  * *d_count (device int64) receives the total number of matches M; only positions p < capacity
  * are written, so the call succeeded iff M <= capacity (read *d_count after the stream).
+ * A negative *d_count means a bounded device wait of the DIRECT_TMA kernel ran out (report it as
+ * SJ_ERR_TIMEOUT; the outputs are incomplete).
  * A DISTINCT table never has M > probe rows. Output order is unspecified, as cuDF's is.
  * Stream-ordered; scratch for GROUPED tables comes from `alloc`. */
 SJ_EXPORT sj_status sj_probe_gather(const sj_table* table, const sj_column* probe_keys,

@@ -215,6 +215,8 @@ class HashTable:
             out.count = -1
             return out
         out.count = int(dc.item())
+        if out.count < 0:
+            raise L.SjError(L.SJ_ERR_TIMEOUT, "sj_probe_gather", "a bounded device wait ran out")
         if out.count > capacity:
             raise L.SjError(L.SJ_ERR_CAPACITY, "sj_probe_gather", f"{out.count} matches > capacity {capacity}")
         return out

@@ -274,6 +274,28 @@ __global__ void __launch_bounds__(256) group_scatter_kernel(TableDev t, const K*
 
 static int bit_width_u64(uint64_t v) { return v ? 64 - __builtin_clzll(v) : 0; }
 
+// Row store of a GROUPED table, rewritten in group order: dst record i = src record idx[i]
+// (records of `stride` bytes, a multiple of 4), so a probe expanding a group reads its members'
+// records contiguously instead of through a position list.
+__global__ void __launch_bounds__(256) permute_records_kernel(const char* __restrict__ src, char* __restrict__ dst,
+                                                              const int32_t* __restrict__ idx, int64_t n,
+                                                              int stride) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const char* a = src + (int64_t)__ldg(idx + i) * stride;
+    char* b = dst + i * stride;
+    if (stride % 16 == 0) {
+      for (int o = 0; o < stride; o += 16)
+        *reinterpret_cast<uint4*>(b + o) = __ldg(reinterpret_cast<const uint4*>(a + o));
+    } else if (stride % 8 == 0) {
+      for (int o = 0; o < stride; o += 8)
+        *reinterpret_cast<uint2*>(b + o) = __ldg(reinterpret_cast<const uint2*>(a + o));
+    } else {
+      for (int o = 0; o < stride; o += 4)
+        *reinterpret_cast<uint32_t*>(b + o) = __ldg(reinterpret_cast<const uint32_t*>(a + o));
+    }
+  }
+}
+
 static TableDev make_dev(const sj_table* t) {
   TableDev d{};
   d.slots = t->slots;
@@ -596,6 +618,27 @@ sj_status build_table(const sj_column& keys, const sj_column* payload, int32_t n
       return fail(set_error(SJ_ERR_DEVICE, std::string("grouped build: ") + cudaGetErrorString(cudaGetLastError())));
     if (h.full) return fail(set_error(SJ_ERR_TABLE_FULL, "a table segment ran out of slots"));
     t->max_group = (int32_t)std::max<unsigned>(h.max_group, 1u);
+    if (t->arow && grouped_rows > 0) {
+      // positions become group-order indices: the row store is rewritten in group order and the
+      // position list (now the identity) is dropped
+      void* arow2 = nullptr;
+      if (sj_status e = alloc.allocate(&arow2, t->arow_bytes, stream)) return fail(e);
+      const int g3 = grid_for(t->device, p, grouped_rows, 256);
+      permute_records_kernel<<<g3, 256, 0, stream>>>(static_cast<const char*>(t->arow), static_cast<char*>(arow2),
+                                                     t->grp_rid, grouped_rows, t->arow_stride);
+      char* o = static_cast<char*>(t->arow);
+      char* nw = static_cast<char*>(arow2);
+      t->pos_rid = reinterpret_cast<int32_t*>(nw + (reinterpret_cast<char*>(t->pos_rid) - o));
+      for (int c = 0; c < n_payload; ++c) {
+        t->apay[c] = nw + (static_cast<char*>(t->apay[c]) - o);
+        if (t->apay_valid[c]) t->apay_valid[c] = reinterpret_cast<uint8_t*>(nw + (reinterpret_cast<char*>(t->apay_valid[c]) - o));
+      }
+      alloc.release(t->arow, t->arow_bytes, stream);
+      t->arow = arow2;
+      alloc.release(t->grp_rid, t->grp_rid_bytes, stream);
+      t->grp_rid = nullptr;
+      t->grp_rid_bytes = 0;
+    }
   }
   SJ_CUDA_TRY(cudaGetLastError());
   *out = t;

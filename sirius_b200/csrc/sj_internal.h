@@ -103,7 +103,8 @@ struct sj_table {
   size_t slots_bytes = 0;
   int32_t* grp_off   = nullptr;  // GROUPED: #slots + 2 offsets (group #slots = NULL keys)
   size_t grp_off_bytes = 0;
-  int32_t* grp_rid   = nullptr;  // GROUPED: table positions ordered by group
+  int32_t* grp_rid   = nullptr;  // GROUPED: table positions ordered by group; NULL when the row
+                                  // store is in group order (position = index in group order)
   size_t grp_rid_bytes = 0;
   // Table positions. A slot's row-id field holds a position; the build row id of position p is
   // the int32 at pos_rid + p * pos_stride bytes (pos_rid NULL: positions are the row ids). With

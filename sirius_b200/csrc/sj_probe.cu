@@ -433,6 +433,23 @@ __device__ __forceinline__ int64_t upper_index(const int64_t* off, int64_t lo, i
   return lo;
 }
 
+// Largest e in [e, hi] with off[e] <= j, starting from a known e with off[e] <= j: gallop forward
+// (1, 2, 4, ... entries) then bisect, so a thread whose next position is in the same or a nearby
+// group pays one or two comparisons instead of a full binary search.
+__device__ __forceinline__ int gallop_index(const int64_t* off, int e, int hi, int64_t j) {
+  int step = 1, lo = e;
+  while (lo + step <= hi && off[lo + step] <= j) {
+    lo += step;
+    step <<= 1;
+  }
+  const int top = lo + step <= hi ? lo + step - 1 : hi;
+  return (int)upper_index(off, lo, top, j);
+}
+
+// Thread t of a tile handles positions j0 + m*256 + t (m < 8: consecutive lanes write consecutive
+// positions). Entry lookups stay in shared memory; then every item's group-member load is issued,
+// then every item's record (or row id + payloads), then the stores — 8 independent load chains per
+// thread instead of one at a time.
 __global__ void __launch_bounds__(kExpandThreads) expand_kernel(const int32_t* __restrict__ m_row,
                                                                 const int32_t* __restrict__ m_start,
                                                                 const int64_t* __restrict__ m_off,
@@ -459,49 +476,99 @@ __global__ void __launch_bounds__(kExpandThreads) expand_kernel(const int32_t* _
   for (int64_t tile = t_lo; tile < t_hi; ++tile) {
     const int64_t j0 = tile * kExpandTile;
     const int64_t j1 = j0 + kExpandTile < cap ? j0 + kExpandTile : cap;
-    const int64_t ne = (nent - e0) < (kExpandTile + 1) ? (nent - e0) : (kExpandTile + 1);
+    const int ne = (int)((nent - e0) < (kExpandTile + 1) ? (nent - e0) : (kExpandTile + 1));
     for (int i = threadIdx.x; i < ne; i += kExpandThreads) {
       s_off[i] = m_off[e0 + i];
       s_row[i] = m_row[e0 + i];
       s_start[i] = m_start[e0 + i];
     }
     __syncthreads();
-#pragma unroll 1
+    // 1. entries (shared memory only)
+    int32_t row[kExpandItems], gi[kExpandItems];
+    int e = 0;
+#pragma unroll
     for (int m = 0; m < kExpandItems; ++m) {
       const int64_t j = j0 + (int64_t)m * kExpandThreads + threadIdx.x;
-      const bool live = j < j1;
-      int32_t row = 0, pos = 0, rid = 0;
-      if (live) {
-        const int64_t e = upper_index(s_off, 0, ne - 1, j);
-        row = s_row[e];
-        pos = __ldg(grp_rid + s_start[e] + (j - s_off[e]));
-        rid = brid_of(g, pos);
-        if (g.out_prid) __stcs(g.out_prid + j, row);
-        if (g.out_brid) __stcs(g.out_brid + j, rid);
+      row[m] = 0;
+      gi[m] = -1;
+      if (j < j1) {
+        e = m == 0 ? (int)upper_index(s_off, 0, ne - 1, j) : gallop_index(s_off, e, ne - 1, j);
+        row[m] = s_row[e];
+        gi[m] = s_start[e] + (int32_t)(j - s_off[e]);
       }
-      for (int c = 0; c < g.n_pin; ++c) {
-        const PayloadIn in = g.pin[c];
-        bool v = false;
-        if (live) {
-          store_elem_cs(g.pout[c].data, j, in.width, pl_load(in, row));
-          v = payload_valid(in, row);
+    }
+    // 2. group members (table positions)
+    int32_t pos[kExpandItems];
+#pragma unroll
+    for (int m = 0; m < kExpandItems; ++m) pos[m] = gi[m] < 0 ? 0 : grp_rid ? __ldg(grp_rid + gi[m]) : gi[m];
+    // 3. build side: one row-store record per item, or row id (+ payloads by row id / position)
+    if (g.rec) {
+      constexpr int kHalf = kExpandItems / 2;  // 4 records (up to 32 registers) in flight at a time
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        Record r[kHalf];
+#pragma unroll
+        for (int q = 0; q < kHalf; ++q) {
+          const int m = h * kHalf + q;
+          if (gi[m] >= 0)
+            r[q] = load_record(static_cast<const char*>(g.rec) + (int64_t)pos[m] * g.rec_stride, g.rec_stride);
         }
+#pragma unroll
+        for (int q = 0; q < kHalf; ++q) {
+          const int m = h * kHalf + q;
+          const int64_t j = j0 + (int64_t)m * kExpandThreads + threadIdx.x;
+          const bool live = gi[m] >= 0;
+          if (live && g.out_prid) __stcs(g.out_prid + j, row[m]);
+          if (live && g.out_brid) __stcs(g.out_brid + j, (int32_t)r[q].w[0]);
+          for (int c = 0; c < g.n_bin; ++c) {
+            const int w = g.bin[c].width;
+            if (live) store_elem_cs(g.bout[c].data, j, w, record_field(r[q], g.rec_off[c], w));
+            if (g.rec_voff[c] >= 0) {
+              const unsigned word = __ballot_sync(kFullMask, live && record_field(r[q], g.rec_voff[c], 1) != 0);
+              if (lane == 0 && j - lane < j1) g.bout[c].valid[(j - lane) >> 5] = word;
+            }
+          }
+        }
+      }
+    } else {
+      int32_t rid[kExpandItems];
+#pragma unroll
+      for (int m = 0; m < kExpandItems; ++m) rid[m] = gi[m] >= 0 ? brid_of(g, pos[m]) : 0;
+#pragma unroll
+      for (int m = 0; m < kExpandItems; ++m) {
+        const int64_t j = j0 + (int64_t)m * kExpandThreads + threadIdx.x;
+        const bool live = gi[m] >= 0;
+        if (live && g.out_prid) __stcs(g.out_prid + j, row[m]);
+        if (live && g.out_brid) __stcs(g.out_brid + j, rid[m]);
+        for (int c = 0; c < g.n_bin; ++c) {
+          const PayloadIn in = g.bin[c];
+          const int32_t idx = g.bin_by_pos ? pos[m] : rid[m];
+          bool v = false;
+          if (live) {
+            store_elem_cs(g.bout[c].data, j, in.width, pl_load(in, idx));
+            v = payload_valid(in, idx);
+          }
+          if (has_validity(in)) {
+            const unsigned word = __ballot_sync(kFullMask, v);
+            if (lane == 0 && j - lane < j1) g.bout[c].valid[(j - lane) >> 5] = word;
+          }
+        }
+      }
+    }
+    // 4. probe payloads (by probe row)
+    for (int c = 0; c < g.n_pin; ++c) {
+      const PayloadIn in = g.pin[c];
+      uint64_t v[kExpandItems];
+#pragma unroll
+      for (int m = 0; m < kExpandItems; ++m) v[m] = gi[m] >= 0 ? pl_load(in, row[m]) : 0;
+#pragma unroll
+      for (int m = 0; m < kExpandItems; ++m) {
+        const int64_t j = j0 + (int64_t)m * kExpandThreads + threadIdx.x;
+        const bool live = gi[m] >= 0;
+        if (live) store_elem_cs(g.pout[c].data, j, in.width, v[m]);
         if (has_validity(in)) {
-          const unsigned word = __ballot_sync(kFullMask, v);
+          const unsigned word = __ballot_sync(kFullMask, live && payload_valid(in, row[m]));
           if (lane == 0 && j - lane < j1) g.pout[c].valid[(j - lane) >> 5] = word;
-        }
-      }
-      for (int c = 0; c < g.n_bin; ++c) {
-        const PayloadIn in = g.bin[c];
-        const int32_t idx = g.bin_by_pos ? pos : rid;
-        bool v = false;
-        if (live) {
-          store_elem_cs(g.bout[c].data, j, in.width, pl_load(in, idx));
-          v = payload_valid(in, idx);
-        }
-        if (has_validity(in)) {
-          const unsigned word = __ballot_sync(kFullMask, v);
-          if (lane == 0 && j - lane < j1) g.bout[c].valid[(j - lane) >> 5] = word;
         }
       }
     }

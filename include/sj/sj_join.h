@@ -244,6 +244,45 @@ SJ_EXPORT sj_status sj_probe_gather(const sj_table* table, const sj_column* prob
                                     const sj_mut_column* out_build_payload, int64_t capacity,
                                     const sj_alloc* alloc, sj_stream_t stream, int64_t* d_count);
 
+/* Join types of the operator's BUILD_PROBE path on a built table
+ * (src/op/sirius_physical_hash_join.cpp:1640-1700; MARK: resolve_mark_join_result, :1461-1525). */
+typedef enum sj_join_kind {
+  SJ_JOIN_INNER = 0,
+  SJ_JOIN_LEFT = 1,  /* INNER rows + every probe row without a match (NULL keys included) */
+  SJ_JOIN_SEMI = 2,  /* probe rows with at least one match, each once */
+  SJ_JOIN_ANTI = 3,  /* probe rows without a match (NULL keys included: NOT EXISTS) */
+  SJ_JOIN_MARK = 4,  /* one BOOL8 per probe row, SQL three-valued (IN) */
+  SJ_JOIN_FULL = 5   /* LEFT rows + every build row without a match (NULL keys included) */
+} sj_join_kind;
+
+/* Row id written for the missing side of an outer row (cuDF's JoinNoneValue). */
+#define SJ_NO_ROW ((int32_t)0x80000000)
+
+/* A join of `kind` on a built table; the counterpart of sj_probe_gather for every join type.
+ *   INNER: exactly sj_probe_gather.
+ *   LEFT:  the INNER rows at positions [0, M), then one row per unmatched probe row with
+ *          out_build_rid = SJ_NO_ROW and NULL build payloads; every out_build_payload must have a
+ *          validity buffer. *d_count = total rows.
+ *   FULL:  the LEFT rows, then one row per unmatched build row (NULL keys included) with
+ *          out_probe_rid = SJ_NO_ROW and NULL probe payloads; every output payload needs a validity
+ *          buffer, and build payloads must be caller columns (build_payload != NULL), since
+ *          NULL-key build rows are not stored in the table. A FULL join of several probe batches
+ *          would need their matches combined; this call covers one probe input.
+ *   SEMI / ANTI: out_probe_rid and the probe payloads of the selected probe rows (build outputs
+ *          unused). *d_count = rows.
+ *   MARK:  out_mark[i] = 1 if probe row i has a match, else 0, for every probe row; out_mark_validity
+ *          (bitmask, may be NULL only when no row can be NULL) marks NULL the unmatched rows whose
+ *          probe key is NULL, or every unmatched row when the build side has a NULL key (the IN rule
+ *          of resolve_mark_join_result; the table must use SJ_NULLS_UNEQUAL). *d_count = probe rows.
+ * Rows beyond `capacity` are not written (*d_count still counts them). Stream-ordered. */
+SJ_EXPORT sj_status sj_probe_join(const sj_table* table, sj_join_kind kind, const sj_column* probe_keys,
+                                  int32_t num_keys, const sj_column* probe_payload, int32_t num_probe_payload,
+                                  const sj_column* build_payload, int32_t num_build_payload, int32_t* out_probe_rid,
+                                  int32_t* out_build_rid, const sj_mut_column* out_probe_payload,
+                                  const sj_mut_column* out_build_payload, int64_t capacity, uint8_t* out_mark,
+                                  uint32_t* out_mark_validity, const sj_alloc* alloc, sj_stream_t stream,
+                                  int64_t* d_count);
+
 /* One-shot INNER join (STANDARD mode: cudf::inner_join(left_keys, right_keys, compare_nulls(),
  * stream), src/op/sirius_physical_hash_join.cpp:1872, followed by gather_join_output): builds a
  * throwaway table on build_keys, probes it with probe_keys and gathers. Same output contract as

@@ -9,7 +9,9 @@ Two independent restatements of the semantics of Sirius's INNER hash join
 ``:1299-1359`` for the gathered output columns):
 
 * ``hash_join`` — the multithreaded C chained-hash join in ``oracle.c`` (also the CPU baseline);
-* ``sort_merge_join`` — a numpy sort-merge join, used to cross-check the C oracle.
+* ``sort_merge_join`` — a numpy sort-merge join, used to cross-check the C oracle;
+* ``kind_join`` / ``mark_join`` — LEFT, FULL, SEMI, ANTI and MARK restated from the INNER pairs
+  (``:1640-1700``, ``resolve_mark_join_result`` ``:1461-1525``).
 
 Parity pinning: ``tests/golden/`` restates the known answers of the reference's own join tests
 (``test/cpp/integration/test_gpu_execution_join_nulls.cpp:42-58`` and
@@ -179,6 +181,67 @@ def sort_merge_join(bkeys, pkeys, bvalid=None, pvalid=None, nulls_equal=False):
             prid = np.concatenate([prid, np.repeat(pn, len(bn))])
             brid = np.concatenate([brid, np.tile(bn, len(pn))])
     return prid.astype(np.int32), brid.astype(np.int32)
+
+
+# ------------------------------------------------------------------------------------------------
+# The other join types, restated from the INNER pairs (numpy)
+# ------------------------------------------------------------------------------------------------
+NO_ROW = np.int32(-(1 << 31))  # the missing side of an outer row (cuDF's JoinNoneValue)
+
+
+def kind_join(kind, bkeys, pkeys, bvalid=None, pvalid=None, nulls_equal=False):
+    """Row-id pairs of a LEFT / FULL / SEMI / ANTI join, following the operator's join types
+    (src/op/sirius_physical_hash_join.cpp:1640-1700: filtered_join semi/anti, hash_join left/full):
+    semi = probe rows with a match; anti = the others (NULL keys included: NOT EXISTS);
+    left = INNER pairs + (unmatched probe row, NO_ROW); full = left + (NO_ROW, unmatched build row),
+    NULL-key build rows included. Returns (prid, brid) int32 arrays (brid None for semi/anti)."""
+    pr, br = sort_merge_join(bkeys, pkeys, bvalid, pvalid, nulls_equal=nulls_equal)
+    n_p, n_b = len(pkeys), len(bkeys)
+    p_hit = np.zeros(n_p, bool)
+    p_hit[pr] = True
+    if kind == "semi":
+        return np.nonzero(p_hit)[0].astype(np.int32), None
+    if kind == "anti":
+        return np.nonzero(~p_hit)[0].astype(np.int32), None
+    miss_p = np.nonzero(~p_hit)[0].astype(np.int32)
+    prid = np.concatenate([pr, miss_p])
+    brid = np.concatenate([br, np.full(len(miss_p), NO_ROW, np.int32)])
+    if kind == "left":
+        return prid, brid
+    if kind == "full":
+        b_hit = np.zeros(n_b, bool)
+        b_hit[br] = True
+        miss_b = np.nonzero(~b_hit)[0].astype(np.int32)
+        return (np.concatenate([prid, np.full(len(miss_b), NO_ROW, np.int32)]), np.concatenate([brid, miss_b]))
+    raise ValueError(kind)
+
+
+def mark_join(bkeys, pkeys, bvalid=None, pvalid=None):
+    """MARK join (resolve_mark_join_result, src/op/sirius_physical_hash_join.cpp:1461-1525): for
+    every probe row (mark, valid): mark = it has a match; an unmatched row is NULL when its key is
+    NULL or when the build side has a NULL key (the IN rule; NULLs compare unequal)."""
+    pr, _ = sort_merge_join(bkeys, pkeys, bvalid, pvalid)
+    n_p = len(pkeys)
+    mark = np.zeros(n_p, bool)
+    mark[pr] = True
+    pv = unpack_validity(pvalid, n_p) if pvalid is not None else np.ones(n_p, bool)
+    build_has_null = bvalid is not None and not unpack_validity(bvalid, len(bkeys)).all()
+    valid = mark | (pv if not build_has_null else np.zeros(n_p, bool))
+    return mark, valid
+
+
+def gather_nullable(col, rid, valid=None):
+    """Payload column gathered by row id with NULLs for NO_ROW (and for NULL inputs): (values,
+    validity bool). Values at NULL rows are 0."""
+    rid = np.asarray(rid)
+    ok = rid != NO_ROW
+    v = np.zeros(len(rid), col.dtype)
+    v[ok] = col[rid[ok]]
+    m = ok.copy()
+    if valid is not None:
+        m[ok] &= unpack_validity(valid, len(col))[rid[ok]]
+    v[~m] = 0
+    return v, m
 
 
 # ------------------------------------------------------------------------------------------------

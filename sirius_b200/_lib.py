@@ -22,6 +22,8 @@ SJ_LAYOUT_AUTO, SJ_LAYOUT_DISTINCT, SJ_LAYOUT_GROUPED = 0, 1, 2
 SJ_NULLS_UNEQUAL, SJ_NULLS_EQUAL = 0, 1
 SJ_SLOT_PACKED64, SJ_SLOT_WIDE128 = 0, 1
 SJ_AGG_AUTO, SJ_AGG_WARP, SJ_AGG_CTA = 0, 1, 2
+SJ_JOIN_INNER, SJ_JOIN_LEFT, SJ_JOIN_SEMI, SJ_JOIN_ANTI, SJ_JOIN_MARK, SJ_JOIN_FULL = range(6)
+SJ_NO_ROW = -(1 << 31)
 SJ_PROBE_KERNEL_AUTO, SJ_PROBE_KERNEL_STAGED, SJ_PROBE_KERNEL_DIRECT, SJ_PROBE_KERNEL_DIRECT_TMA = 0, 1, 2, 3
 
 
@@ -103,6 +105,9 @@ SIGNATURES = {
     "sj_inner_join_noalloc": (c_int32, [_P(SjColumn), _P(SjColumn), c_int32, _P(SjColumn), c_int32, _P(SjColumn),
                                         c_int32, c_void_p, c_void_p, _P(SjMutColumn), _P(SjMutColumn), c_int64,
                                         _P(SjJoinParams), c_void_p, c_void_p]),
+    "sj_probe_join": (c_int32, [c_void_p, c_int32, _P(SjColumn), c_int32, _P(SjColumn), c_int32, _P(SjColumn),
+                                c_int32, c_void_p, c_void_p, _P(SjMutColumn), _P(SjMutColumn), c_int64, c_void_p,
+                                c_void_p, _P(SjAlloc), c_void_p, c_void_p]),
     "sj_status_string": (c_char_p, [c_int32]),
     "sj_last_error": (c_char_p, []),
     "sj_version": (c_int32, []),

@@ -242,7 +242,7 @@ SJ_EXPORT sj_status sj_table_get_info(const sj_table* t, sj_table_info* info) {
   info->null_rows = t->null_rows;
   info->distinct_keys = t->distinct;
   info->num_slots = t->num_slots();
-  size_t bytes = t->slots_bytes + t->grp_off_bytes + t->grp_rid_bytes + t->arow_bytes;
+  size_t bytes = t->slots_bytes + t->grp_off_bytes + t->grp_rid_bytes + t->arow_bytes + t->null_rid_bytes;
   if (t->apay_owned)
     for (int c = 0; c < t->n_attached; ++c) bytes += t->apay_bytes[c] + t->apay_valid_bytes[c];
   info->device_bytes = (int64_t)bytes;
@@ -282,6 +282,26 @@ SJ_EXPORT sj_status sj_probe_gather(const sj_table* table, const sj_column* prob
                out_build_rid, out_probe_payload, out_build_payload, capacity};
   try {
     return probe_gather(table, probe_keys[0], g, Allocator(alloc), reinterpret_cast<cudaStream_t>(stream), d_count);
+  } catch (const std::exception& e) {
+    return set_error(SJ_ERR_DEVICE, e.what());
+  }
+}
+
+SJ_EXPORT sj_status sj_probe_join(const sj_table* table, sj_join_kind kind, const sj_column* probe_keys,
+                                  int32_t num_keys, const sj_column* probe_payload, int32_t num_probe_payload,
+                                  const sj_column* build_payload, int32_t num_build_payload, int32_t* out_probe_rid,
+                                  int32_t* out_build_rid, const sj_mut_column* out_probe_payload,
+                                  const sj_mut_column* out_build_payload, int64_t capacity, uint8_t* out_mark,
+                                  uint32_t* out_mark_validity, const sj_alloc* alloc, sj_stream_t stream,
+                                  int64_t* d_count) {
+  clear_error();
+  if (!table || !probe_keys || !d_count) return set_error(SJ_ERR_INVALID, "table, probe_keys and d_count are required");
+  if (num_keys != 1) return set_error(SJ_ERR_INVALID, "exactly one key column is supported");
+  GatherSpec g{probe_payload, num_probe_payload, build_payload, num_build_payload, out_probe_rid,
+               out_build_rid, out_probe_payload, out_build_payload, capacity};
+  try {
+    return probe_join(table, (int32_t)kind, probe_keys[0], g, out_mark, out_mark_validity, Allocator(alloc),
+                      reinterpret_cast<cudaStream_t>(stream), d_count);
   } catch (const std::exception& e) {
     return set_error(SJ_ERR_DEVICE, e.what());
   }

@@ -296,6 +296,23 @@ __global__ void __launch_bounds__(256) permute_records_kernel(const char* __rest
   }
 }
 
+// Row ids of the NULL-key rows (warp-aggregated compaction; order unspecified).
+__global__ void __launch_bounds__(256) null_rows_kernel(const uint32_t* __restrict__ kv, int64_t kvoff, int64_t n,
+                                                        int32_t* out, unsigned long long* count) {
+  const int lane = threadIdx.x & 31;
+  for (int64_t i0 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) & ~31ll; i0 < n;
+       i0 += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t i = i0 + lane;
+    const bool is_null = i < n && !bit_valid(kv, kvoff, i);
+    const unsigned bal = __ballot_sync(kFullMask, is_null);
+    if (!bal) continue;
+    unsigned long long base = 0;
+    if (lane == 0) base = atomicAdd(count, (unsigned long long)__popc(bal));
+    base = __shfl_sync(kFullMask, base, 0);
+    if (is_null) out[base + __popc(bal & ((1u << lane) - 1))] = (int32_t)i;
+  }
+}
+
 static TableDev make_dev(const sj_table* t) {
   TableDev d{};
   d.slots = t->slots;
@@ -640,6 +657,15 @@ sj_status build_table(const sj_column& keys, const sj_column* payload, int32_t n
       t->grp_rid_bytes = 0;
     }
   }
+  if (t->null_rows > 0 && !null_group) {
+    t->null_rid_bytes = (size_t)t->null_rows * sizeof(int32_t);
+    if (sj_status e = alloc.allocate((void**)&t->null_rid, t->null_rid_bytes, stream)) return fail(e);
+    Scratch cnt_buf;
+    if (sj_status e = cnt_buf.get(alloc, sizeof(unsigned long long), stream)) return fail(e);
+    SJ_CUDA_TRY(cudaMemsetAsync(cnt_buf.ptr, 0, sizeof(unsigned long long), stream));
+    null_rows_kernel<<<grid, 256, 0, stream>>>(keys.validity, keys.validity_offset, n, t->null_rid,
+                                               cnt_buf.as<unsigned long long>());
+  }
   SJ_CUDA_TRY(cudaGetLastError());
   *out = t;
   return SJ_OK;
@@ -651,6 +677,7 @@ sj_status destroy_table(sj_table* t, cudaStream_t stream) {
   if (t->grp_off) t->alloc.release(t->grp_off, t->grp_off_bytes, stream);
   if (t->grp_rid) t->alloc.release(t->grp_rid, t->grp_rid_bytes, stream);
   if (t->arow) t->alloc.release(t->arow, t->arow_bytes, stream);
+  if (t->null_rid) t->alloc.release(t->null_rid, t->null_rid_bytes, stream);
   if (t->apay_owned) {
     for (int c = 0; c < t->n_attached; ++c) {
       if (t->apay[c]) t->alloc.release(t->apay[c], t->apay_bytes[c], stream);

@@ -127,6 +127,10 @@ struct sj_table {
   uint8_t* apay_valid[8] = {};
   int32_t apay_vstride[8] = {};
   bool apay_owned    = false;
+  // Row ids of the NULL-key build rows when NULLs never match (they are not in the table; a FULL
+  // join emits them as unmatched rows). Built only when the build has NULL keys.
+  int32_t* null_rid  = nullptr;
+  size_t null_rid_bytes = 0;
   size_t apay_bytes[8] = {};
   size_t apay_valid_bytes[8] = {};
   sj_join_params params{};
@@ -161,5 +165,9 @@ sj_status probe_gather(const sj_table* t, const sj_column& probe, const GatherSp
                        const Allocator& alloc, cudaStream_t stream, int64_t* d_count);
 
 sj_status validate_column(const sj_column* c, const char* what, bool key);
+
+// LEFT / SEMI / ANTI / MARK / FULL (sj_probe_kinds.cu); INNER delegates to probe_gather.
+sj_status probe_join(const sj_table* t, int32_t kind, const sj_column& probe, const GatherSpec& g, uint8_t* out_mark,
+                     uint32_t* out_mark_valid, const Allocator& alloc, cudaStream_t stream, int64_t* d_count);
 
 }  // namespace sj

@@ -77,6 +77,8 @@ class JoinOutput:
     build_payload: list = field(default_factory=list)
     probe_payload_validity: list = field(default_factory=list)
     build_payload_validity: list = field(default_factory=list)
+    mark: Optional[torch.Tensor] = None           # MARK: one uint8 per probe row
+    mark_validity: Optional[torch.Tensor] = None  # MARK: bitmask words
 
     def trimmed(self) -> "JoinOutput":
         n = self.count
@@ -219,6 +221,71 @@ class HashTable:
             raise L.SjError(L.SJ_ERR_TIMEOUT, "sj_probe_gather", "a bounded device wait ran out")
         if out.count > capacity:
             raise L.SjError(L.SJ_ERR_CAPACITY, "sj_probe_gather", f"{out.count} matches > capacity {capacity}")
+        return out
+
+    def probe_join(self, kind: int, probe_keys: torch.Tensor, probe_validity: Optional[torch.Tensor] = None,
+                   probe_payload=(), build_payload=(), *, attached: bool = False, capacity: Optional[int] = None,
+                   stream: Optional[torch.cuda.Stream] = None) -> JoinOutput:
+        """LEFT / SEMI / ANTI / MARK / FULL (``sj_probe_join``; INNER is ``probe_gather``).
+
+        Outer rows carry ``SJ_NO_ROW`` as the missing side's row id and NULL payloads; LEFT/FULL
+        outputs get validity buffers for every padded payload column. Synchronizes."""
+        dev = probe_keys.device
+        n = probe_keys.numel()
+        if kind == L.SJ_JOIN_INNER:
+            return self.probe_gather(probe_keys, probe_validity, probe_payload, build_payload, attached=attached,
+                                     capacity=capacity, stream=stream)
+        if attached:
+            if build_payload:
+                raise ValueError("attached=True gathers the attached build columns; pass no build_payload")
+            build_payload = self.attached
+        out = JoinOutput(0, None, None)
+        if kind == L.SJ_JOIN_MARK:
+            out.mark = torch.empty(n, dtype=torch.uint8, device=dev)
+            out.mark_validity = torch.empty((n + 31) // 32, dtype=torch.int32, device=dev)
+            capacity = 0
+        else:
+            if capacity is None:
+                capacity = n
+                if kind in (L.SJ_JOIN_LEFT, L.SJ_JOIN_FULL):
+                    capacity += int(self.count(probe_keys, probe_validity, stream).item())
+                if kind == L.SJ_JOIN_FULL:
+                    capacity += self.build_rows
+            pad_probe = kind == L.SJ_JOIN_FULL
+            pad_build = kind in (L.SJ_JOIN_LEFT, L.SJ_JOIN_FULL)
+            words = (capacity + 31) // 32
+            out.probe_rid = torch.empty(capacity, dtype=torch.int32, device=dev)
+            out.build_rid = torch.empty(capacity, dtype=torch.int32, device=dev) if pad_build else None
+            for c in probe_payload:
+                t, v = _as_pair(c)
+                out.probe_payload.append(torch.empty(capacity, dtype=t.dtype, device=dev))
+                out.probe_payload_validity.append(
+                    torch.empty(words, dtype=torch.int32, device=dev) if (v is not None or pad_probe) else None)
+            if pad_build:
+                for c in build_payload:
+                    t, _ = _as_pair(c)
+                    out.build_payload.append(torch.empty(capacity, dtype=t.dtype, device=dev))
+                    out.build_payload_validity.append(torch.empty(words, dtype=torch.int32, device=dev))
+        pin = [make_column(*_as_pair(c)) for c in probe_payload]
+        use_build = kind in (L.SJ_JOIN_LEFT, L.SJ_JOIN_FULL)
+        bin_ = [] if (attached or not use_build) else [make_column(*_as_pair(c)) for c in build_payload]
+        n_bin = len(build_payload) if use_build else 0
+        pout = [_mut(t, v) for t, v in zip(out.probe_payload, out.probe_payload_validity)]
+        bout = [_mut(t, v) for t, v in zip(out.build_payload, out.build_payload_validity)]
+        dc = torch.empty(1, dtype=torch.int64, device=dev)
+        key = make_column(probe_keys, probe_validity)
+        st = self._lib.sj_probe_join(
+            self.handle, kind, ctypes.byref(key), 1, _cols(pin), len(pin), None if attached else _cols(bin_), n_bin,
+            out.probe_rid.data_ptr() if out.probe_rid is not None else None,
+            out.build_rid.data_ptr() if out.build_rid is not None else None,
+            _cols(pout, L.SjMutColumn), _cols(bout, L.SjMutColumn), capacity,
+            out.mark.data_ptr() if out.mark is not None else None,
+            out.mark_validity.data_ptr() if out.mark_validity is not None else None, None, _stream_handle(stream),
+            dc.data_ptr())
+        L.check(st, "sj_probe_join")
+        out.count = int(dc.item())
+        if kind != L.SJ_JOIN_MARK and out.count > capacity:
+            raise L.SjError(L.SJ_ERR_CAPACITY, "sj_probe_join", f"{out.count} rows > capacity {capacity}")
         return out
 
     def close(self, stream: Optional[torch.cuda.Stream] = None):

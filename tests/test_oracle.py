@@ -128,3 +128,57 @@ def test_empty_sides():
     assert O.hash_join_count(e32, np.array([1, 2], np.int32)) == 0
     assert O.hash_join_count(np.array([1, 2], np.int32), e32) == 0
     assert O.hash_join(e32, e32).rows == 0
+
+
+def _pairs(pr, br, lid, rid):
+    key = lambda x: (x[0] is None, x[0] or 0, x[1] is None, x[1] or 0)  # noqa: E731
+    return sorted([(None if p == O.NO_ROW else int(lid[p]), None if b == O.NO_ROW else int(rid[b]))
+                   for p, b in zip(pr, br)], key=key)
+
+
+@pytest.mark.parametrize("kind", ["left", "full"])
+def test_outer_known_answers(kind):
+    fx, lk, lv, rk, rv, lid, rid = _fixture()
+    pr, br = O.kind_join(kind, rk, lk, rv, lv)
+    exp = sorted([tuple(p) for p in fx[kind]], key=lambda x: (x[0] is None, x[0] or 0, x[1] is None, x[1] or 0))
+    assert _pairs(pr, br, lid, rid) == exp
+
+
+@pytest.mark.parametrize("kind", ["semi", "anti"])
+def test_semi_anti_known_answers(kind):
+    fx, lk, lv, rk, rv, lid, rid = _fixture()
+    pr, _ = O.kind_join(kind, rk, lk, rv, lv)
+    assert sorted(lid[pr].tolist()) == fx[kind]
+
+
+def test_mark_known_answers():
+    fx, lk, lv, rk, rv, lid, rid = _fixture()
+    m, v = O.mark_join(rk, lk, rv, lv)
+    assert [[int(lid[i]), bool(m[i]) if v[i] else None] for i in range(len(lk))] == fx["mark_with_null_build"]
+    keep = np.array([k is not None for k in fx["r"]["k"]])
+    m, v = O.mark_join(rk[keep], lk, None, lv)
+    assert [[int(lid[i]), bool(m[i]) if v[i] else None] for i in range(len(lk))] == fx["mark_null_free_build"]
+
+
+@pytest.mark.parametrize("case", GOLDEN["mark_cases"], ids=lambda c: c["name"])
+def test_mark_cases(case):
+    lk, lv = _col(case["left"])
+    rk, rv = _col(case["right"]) if case["right"] else (np.zeros(0, np.int32), None)
+    m, v = O.mark_join(rk, lk, rv, lv)
+    assert [bool(m[i]) if v[i] else None for i in range(len(lk))] == case["mark"]
+
+
+def test_kind_join_partitions_the_probe_rows():
+    """semi + anti = every probe row once; left rows = inner rows + anti rows."""
+    rng = np.random.default_rng(5)
+    bk = rng.integers(0, 300, 1000).astype(np.int64)
+    pk = rng.integers(-20, 400, 4000).astype(np.int64)
+    bv = O.pack_validity(rng.random(1000) > 0.1)
+    pv = O.pack_validity(rng.random(4000) > 0.1)
+    s, _ = O.kind_join("semi", bk, pk, bv, pv)
+    a, _ = O.kind_join("anti", bk, pk, bv, pv)
+    assert np.array_equal(np.sort(np.concatenate([s, a])), np.arange(4000))
+    pr, br = O.kind_join("left", bk, pk, bv, pv)
+    assert len(pr) == O.hash_join_count(bk, pk, bv, pv) + len(a)
+    pr, br = O.kind_join("full", bk, pk, bv, pv)
+    assert np.all(np.isin(np.arange(1000), br))  # every build row appears in a FULL join

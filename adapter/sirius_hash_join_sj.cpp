@@ -1,10 +1,13 @@
 // Sirius-side glue for the sm_100a equi-join (see sirius_hash_join_sj.hpp).
 //
-// Call sites it replaces in src/op/sirius_physical_hash_join.cpp (INNER joins):
+// Call sites it replaces in src/op/sirius_physical_hash_join.cpp:
 //   build   :1614-1615 / :1852 cudf::distinct_hash_join(...)  -> sj_hash_table(..., unique=true)
 //           :1620          cudf::hash_join(...)              -> sj_hash_table(..., unique=false)
 //   probe   :1671 / :1688 / :1872 inner_join(...)            -> sj_hash_table::inner_join(...)
-//   gather  :1945-1954 gather_join_output(...)               -> (fused into inner_join above)
+//           left_join / semi_join / anti_join (:1640-1700)    -> sj_hash_table::join(kind, ...)
+//           full_join                                         -> sj_hash_table::full_join(...)
+//           semi_join + resolve_mark_join_result (:1461-1525) -> sj_hash_table::mark_join(...)
+//   gather  :1945-1954 gather_join_output(...)               -> (fused into the calls above)
 #include "sirius_hash_join_sj.hpp"
 
 #include <cuda_runtime_api.h>
@@ -133,24 +136,58 @@ std::unique_ptr<cudf::table> sj_hash_table::inner_join(cudf::table_view const& p
                                                        rmm::cuda_stream_view stream,
                                                        rmm::device_async_resource_ref mr) const
 {
+  return run(SJ_JOIN_INNER, probe_keys, probe_payload, nullptr, stream, mr);
+}
+
+std::unique_ptr<cudf::table> sj_hash_table::join(sj_join_kind kind, cudf::table_view const& probe_keys,
+                                                 cudf::table_view const& probe_payload,
+                                                 rmm::cuda_stream_view stream,
+                                                 rmm::device_async_resource_ref mr) const
+{
+  if (kind == SJ_JOIN_MARK) return mark_join(probe_keys, probe_payload, stream, mr);
+  if (kind == SJ_JOIN_FULL) throw std::runtime_error("sj adapter: FULL needs the build columns (full_join)");
+  return run(kind, probe_keys, probe_payload, nullptr, stream, mr);
+}
+
+std::unique_ptr<cudf::table> sj_hash_table::full_join(cudf::table_view const& probe_keys,
+                                                      cudf::table_view const& probe_payload,
+                                                      cudf::table_view const& build_payload,
+                                                      rmm::cuda_stream_view stream,
+                                                      rmm::device_async_resource_ref mr) const
+{
+  return run(SJ_JOIN_FULL, probe_keys, probe_payload, &build_payload, stream, mr);
+}
+
+std::unique_ptr<cudf::table> sj_hash_table::run(sj_join_kind kind, cudf::table_view const& probe_keys,
+                                                cudf::table_view const& probe_payload,
+                                                cudf::table_view const* build_cols, rmm::cuda_stream_view stream,
+                                                rmm::device_async_resource_ref mr) const
+{
   if (probe_keys.num_columns() != 1) throw std::runtime_error("sj adapter: one equi-key column");
   const sj_column key = to_sj(probe_keys.column(0));
   rmm_alloc_ctx ctx{mr};
   const sj_alloc a{&ctx, rmm_alloc, rmm_free};
+  const bool outer_build = kind == SJ_JOIN_LEFT || kind == SJ_JOIN_FULL;  // build side NULL-padded
+  const bool outer_probe = kind == SJ_JOIN_FULL;                          // probe side NULL-padded
+  const bool with_build  = kind == SJ_JOIN_INNER || outer_build;
 
-  // output size: a DISTINCT table never returns more rows than it is probed with; otherwise count
+  // output size: INNER matches (a DISTINCT table never returns more than it is probed with), plus
+  // every probe row for LEFT/SEMI/ANTI, plus every build row for FULL
   sj_table_info info{};
   check(sj_table_get_info(table_, &info), "sj_table_get_info");
   rmm::device_buffer d_count(sizeof(int64_t), stream, mr);
-  int64_t capacity = key.num_rows;
-  if (info.layout != SJ_LAYOUT_DISTINCT) {
+  int64_t inner = key.num_rows;
+  if (info.layout != SJ_LAYOUT_DISTINCT && kind != SJ_JOIN_SEMI && kind != SJ_JOIN_ANTI) {
     check(sj_probe_count(table_, &key, 1, &a, raw(stream), static_cast<int64_t*>(d_count.data())), "sj_probe_count");
-    cudaMemcpyAsync(&capacity, d_count.data(), sizeof(int64_t), cudaMemcpyDeviceToHost, stream.value());
+    cudaMemcpyAsync(&inner, d_count.data(), sizeof(int64_t), cudaMemcpyDeviceToHost, stream.value());
     cudaStreamSynchronize(stream.value());
   }
+  int64_t capacity = kind == SJ_JOIN_INNER ? inner : kind == SJ_JOIN_SEMI || kind == SJ_JOIN_ANTI ? key.num_rows
+                                                                                                  : inner + key.num_rows;
+  if (kind == SJ_JOIN_FULL) capacity += info.build_rows;
 
   // outputs: [probe payload columns..., build payload columns...] plus their null masks
-  std::vector<sj_column> pin;
+  std::vector<sj_column> pin, bin;
   std::vector<rmm::device_buffer> data, masks;
   std::vector<cudf::data_type> types;
   std::vector<sj_mut_column> pout, bout;
@@ -168,18 +205,26 @@ std::unique_ptr<cudf::table> sj_hash_table::inner_join(cudf::table_view const& p
   };
   for (cudf::size_type c = 0; c < probe_payload.num_columns(); ++c) {
     pin.push_back(to_sj(probe_payload.column(c)));
-    add_out(probe_payload.column(c).type(), probe_payload.column(c).nullable(), pout);
+    add_out(probe_payload.column(c).type(), outer_probe || probe_payload.column(c).nullable(), pout);
   }
-  for (size_t c = 0; c < build_types_.size(); ++c) add_out(build_types_[c], build_nullable_[c], bout);
+  if (with_build && build_cols) {
+    for (cudf::size_type c = 0; c < build_cols->num_columns(); ++c) {
+      bin.push_back(to_sj(build_cols->column(c)));
+      add_out(build_cols->column(c).type(), true, bout);
+    }
+  } else if (with_build) {
+    for (size_t c = 0; c < build_types_.size(); ++c) add_out(build_types_[c], outer_build || build_nullable_[c], bout);
+  }
 
-  check(sj_probe_gather(table_, &key, 1, pin.data(), (int32_t)pin.size(), /*attached build payloads*/ nullptr,
-                        (int32_t)bout.size(), nullptr, nullptr, pout.data(), bout.data(), capacity, &a, raw(stream),
-                        static_cast<int64_t*>(d_count.data())),
-        "sj_probe_gather");
+  check(sj_probe_join(table_, kind, &key, 1, pin.data(), (int32_t)pin.size(),
+                      build_cols ? bin.data() : nullptr /* NULL: the attached build columns */, (int32_t)bout.size(),
+                      nullptr, nullptr, pout.data(), bout.data(), capacity, nullptr, nullptr, &a, raw(stream),
+                      static_cast<int64_t*>(d_count.data())),
+        "sj_probe_join");
   int64_t rows = 0;
   cudaMemcpyAsync(&rows, d_count.data(), sizeof(int64_t), cudaMemcpyDeviceToHost, stream.value());
   cudaStreamSynchronize(stream.value());
-  if (rows > capacity) throw std::runtime_error("sj adapter: probe produced more rows than counted");
+  if (rows > capacity) throw std::runtime_error("sj adapter: the join produced more rows than counted");
 
   std::vector<std::unique_ptr<cudf::column>> cols;
   for (size_t c = 0; c < data.size(); ++c) {
@@ -190,6 +235,32 @@ std::unique_ptr<cudf::table> sj_hash_table::inner_join(cudf::table_view const& p
                                         : 0;
     cols.push_back(std::make_unique<cudf::column>(types[c], n, std::move(data[c]), std::move(masks[c]), nc));
   }
+  return std::make_unique<cudf::table>(std::move(cols), stream);
+}
+
+std::unique_ptr<cudf::table> sj_hash_table::mark_join(cudf::table_view const& probe_keys,
+                                                      cudf::table_view const& probe_payload,
+                                                      rmm::cuda_stream_view stream,
+                                                      rmm::device_async_resource_ref mr) const
+{
+  if (probe_keys.num_columns() != 1) throw std::runtime_error("sj adapter: one equi-key column");
+  const sj_column key = to_sj(probe_keys.column(0));
+  rmm_alloc_ctx ctx{mr};
+  const sj_alloc a{&ctx, rmm_alloc, rmm_free};
+  const auto n = static_cast<cudf::size_type>(key.num_rows);
+  rmm::device_buffer d_count(sizeof(int64_t), stream, mr);
+  rmm::device_buffer mark((size_t)n, stream, mr);
+  rmm::device_buffer mask((size_t)((n + 31) / 32) * sizeof(uint32_t), stream, mr);
+  check(sj_probe_join(table_, SJ_JOIN_MARK, &key, 1, nullptr, 0, nullptr, 0, nullptr, nullptr, nullptr, nullptr, 0,
+                      static_cast<uint8_t*>(mark.data()), static_cast<uint32_t*>(mask.data()), &a, raw(stream),
+                      static_cast<int64_t*>(d_count.data())),
+        "sj_probe_join");
+  std::vector<std::unique_ptr<cudf::column>> cols;
+  for (cudf::size_type c = 0; c < probe_payload.num_columns(); ++c)
+    cols.push_back(std::make_unique<cudf::column>(probe_payload.column(c), stream, mr));
+  const cudf::size_type nc = cudf::null_count(static_cast<cudf::bitmask_type const*>(mask.data()), 0, n, stream);
+  cols.push_back(std::make_unique<cudf::column>(cudf::data_type(cudf::type_id::BOOL8), n, std::move(mark),
+                                                std::move(mask), nc));
   return std::make_unique<cudf::table>(std::move(cols), stream);
 }
 

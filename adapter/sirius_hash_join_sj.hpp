@@ -1,5 +1,6 @@
 // Sirius-side glue for the sm_100a equi-join: what `sirius_physical_hash_join::execute`
-// (src/op/sirius_physical_hash_join.cpp:1527-1955) calls instead of cuDF for INNER joins.
+// (src/op/sirius_physical_hash_join.cpp:1527-1955) calls instead of cuDF for its equi-joins
+// (INNER, LEFT, SEMI, ANTI, MARK, FULL on one key column).
 //
 // It maps cudf::column_view to sj_column, wraps the task's RMM resource as an sj_alloc (so the
 // join's device memory is charged to the task's cuCascade reservation,
@@ -48,7 +49,30 @@ class sj_hash_table {
   std::unique_ptr<cudf::table> inner_join(cudf::table_view const& probe_keys, cudf::table_view const& probe_payload,
                                           rmm::cuda_stream_view stream, rmm::device_async_resource_ref mr) const;
 
+  /// The other BUILD_PROBE join types on this table (:1640-1700) with their gather:
+  /// SJ_JOIN_LEFT -> [probe payload..., build payload (NULL where unmatched)...] (hash_join::left_join,
+  /// distinct_hash_join::left_join + gather_distinct_left_join_output); SJ_JOIN_SEMI / SJ_JOIN_ANTI ->
+  /// [probe payload...] (filtered_join::semi_join / anti_join + gather_join_output).
+  std::unique_ptr<cudf::table> join(sj_join_kind kind, cudf::table_view const& probe_keys,
+                                    cudf::table_view const& probe_payload, rmm::cuda_stream_view stream,
+                                    rmm::device_async_resource_ref mr) const;
+
+  /// FULL (hash_join::full_join + gather): the build columns come from the slot's retained build batch
+  /// (right_full.select(rhs_output_columns)), since NULL-key build rows are not in the table.
+  std::unique_ptr<cudf::table> full_join(cudf::table_view const& probe_keys, cudf::table_view const& probe_payload,
+                                         cudf::table_view const& build_payload, rmm::cuda_stream_view stream,
+                                         rmm::device_async_resource_ref mr) const;
+
+  /// MARK (resolve_mark_join_result, :1461-1525): the probe columns, copied, plus a BOOL8 mark with
+  /// SQL three-valued NULLs. The table must have been built with NULLs unequal.
+  std::unique_ptr<cudf::table> mark_join(cudf::table_view const& probe_keys, cudf::table_view const& probe_payload,
+                                         rmm::cuda_stream_view stream, rmm::device_async_resource_ref mr) const;
+
  private:
+  std::unique_ptr<cudf::table> run(sj_join_kind kind, cudf::table_view const& probe_keys,
+                                   cudf::table_view const& probe_payload, cudf::table_view const* build_cols,
+                                   rmm::cuda_stream_view stream, rmm::device_async_resource_ref mr) const;
+
   sj_table* table_ = nullptr;
   std::vector<cudf::data_type> build_types_;
   std::vector<bool> build_nullable_;

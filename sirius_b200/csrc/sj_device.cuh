@@ -162,6 +162,26 @@ struct SlotOps<false> {
   __device__ __forceinline__ static bool match_s(const Bucket& bk, int q, uint64_t ks, uint64_t kmask) {
     return (bk.a[q] & kmask) == ks;
   }
+  // DISTINCT tables: a key occupies at most one slot, so the bucket is tested as a whole (32-bit
+  // halves: rid_bits <= 31, so the row-id field lies in the low word) and the walk may stop once the
+  // bucket's last slot is EMPTY (slots fill in order).
+  __device__ __forceinline__ static bool match_distinct(const Bucket& bk, uint64_t ks, uint64_t kmask,
+                                                        uint32_t rbits, int32_t& pos) {
+    const uint32_t khi = (uint32_t)(ks >> 32), klo = (uint32_t)ks;
+    const uint32_t mhi = (uint32_t)(kmask >> 32), mlo = (uint32_t)kmask;
+    bool any = false;
+    uint32_t sel = 0;
+#pragma unroll
+    for (int q = 0; q < kSlots; ++q) {
+      const uint32_t hi = (uint32_t)(bk.a[q] >> 32), lo = (uint32_t)bk.a[q];
+      const bool m = ((hi & mhi) == khi) & ((lo & mlo) == klo);
+      sel = m ? lo : sel;
+      any |= m;
+    }
+    pos = (int32_t)(sel & ((1u << rbits) - 1u));
+    return any;
+  }
+  __device__ __forceinline__ static bool open(const Bucket& bk) { return bk.a[kSlots - 1] == kEmpty; }
 };
 
 template <>
@@ -178,6 +198,14 @@ struct SlotOps<true> {
   __device__ __forceinline__ static bool match_s(const Bucket& bk, int q, uint64_t kb, uint64_t) {
     return bk.a[2 * q + 1] != kEmpty && bk.a[2 * q] == kb;
   }
+  __device__ __forceinline__ static bool match_distinct(const Bucket& bk, uint64_t kb, uint64_t, uint32_t,
+                                                        int32_t& pos) {
+    const bool m0 = bk.a[1] != kEmpty && bk.a[0] == kb;
+    const bool m1 = bk.a[3] != kEmpty && bk.a[2] == kb;
+    pos = (int32_t)(m0 ? bk.a[1] : bk.a[3]);
+    return m0 | m1;
+  }
+  __device__ __forceinline__ static bool open(const Bucket& bk) { return bk.a[3] == kEmpty; }
 };
 
 // 128-bit compare-and-swap (PTX atom.cas.b128, sm_90+). Returns the previous 16 bytes.

@@ -75,28 +75,31 @@ __global__ void __launch_bounds__(kDirectThreads, (R <= 2 ? 4 : 2))
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
   const unsigned below = (1u << lane) - 1u;
-  const int64_t n = d_n ? *d_n : n_host;
-  constexpr int64_t kRowsCta = (int64_t)kDirectThreads * R;
-  const int64_t tiles = (n + kRowsCta - 1) / kRowsCta;
+  // 32-bit row and position arithmetic: probe rows < 2^31 (the int32 row-id range), and a DISTINCT
+  // probe never has more matches than rows
+  const uint32_t n = (uint32_t)(d_n ? *d_n : n_host);
+  const uint32_t cap = (uint32_t)(a.capacity < (int64_t)n ? a.capacity : (int64_t)n);
+  constexpr uint32_t kRowsCta = (uint32_t)kDirectThreads * R;
+  const uint32_t tiles = (n + kRowsCta - 1) / kRowsCta;
   const uint64_t kmask = ~((1ull << t.rbits) - 1);
-  const int64_t lane_off = (int64_t)warp * (32 * R) + lane;  // row of group j: tile start + lane_off + 32 j
-  __shared__ int64_t s_next;
+  const uint32_t lane_off = (uint32_t)warp * (32 * R) + lane;  // row of group j: tile start + lane_off + 32 j
+  __shared__ uint32_t s_next;
   K k[R];
 #pragma unroll
   for (int j = 0; j < R; ++j) {
-    const int64_t r = (int64_t)blockIdx.x * kRowsCta + lane_off + 32 * j;
+    const uint32_t r = blockIdx.x * kRowsCta + lane_off + 32 * j;
     k[j] = r < n ? __ldcs(keys + r) : (K)0;
   }
   // Tiles: the first two of a CTA are static (blockIdx.x, + gridDim.x); with CTA reservation the
   // later ones come from a shared tile counter, so the CTAs sweep the (partition-ordered) probe
   // rows together and the table rows in use stay one partition's worth, resident in L2.
-  int64_t tile = blockIdx.x, nxt = tile + gridDim.x;
+  uint32_t tile = blockIdx.x, nxt = tile + gridDim.x;
   while (tile < tiles) {
-    const int64_t r0 = tile * kRowsCta + lane_off;
+    const uint32_t r0 = tile * kRowsCta + lane_off;
     uint32_t act = 0;
 #pragma unroll
     for (int j = 0; j < R; ++j) {
-      const int64_t r = r0 + 32 * j;
+      const uint32_t r = r0 + 32 * j;
       if (r < n && bit_valid(kv, kvoff, r) && in_range(t, k[j])) act |= 1u << j;
     }
     uint32_t b[R];
@@ -110,7 +113,7 @@ __global__ void __launch_bounds__(kDirectThreads, (R <= 2 ? 4 : 2))
     // the next tile's keys load while this tile probes, gathers and writes
 #pragma unroll
     for (int j = 0; j < R; ++j) {
-      const int64_t r = nxt * kRowsCta + lane_off + 32 * j;
+      const uint32_t r = nxt * kRowsCta + lane_off + 32 * j;
       k[j] = r < n ? __ldcs(keys + r) : (K)0;
     }
     int32_t pos[R];
@@ -125,17 +128,13 @@ __global__ void __launch_bounds__(kDirectThreads, (R <= 2 ? 4 : 2))
 #pragma unroll
       for (int j = 0; j < R; ++j) {
         if (!(act >> j & 1u)) continue;
-        bool done = false;
-#pragma unroll
-        for (int q = 0; q < Ops::kSlots; ++q) {
-          if (!done && Ops::match_s(bk[j], q, ks[j], kmask)) {
-            pos[j] = Ops::rid(bk[j], q, t.rbits);
-            hit |= 1u << j;
-            done = true;
-          }
-          done |= Ops::empty(bk[j], q);
+        int32_t pj;
+        const bool m = Ops::match_distinct(bk[j], ks[j], kmask, t.rbits, pj);
+        if (m) {
+          pos[j] = pj;
+          hit |= 1u << j;
         }
-        if (done) act &= ~(1u << j);
+        if (m || Ops::open(bk[j])) act &= ~(1u << j);
         else b[j] = next_bucket(b[j], t.segmask);
       }
     }
@@ -152,14 +151,14 @@ __global__ void __launch_bounds__(kDirectThreads, (R <= 2 ? 4 : 2))
 #pragma unroll
       for (int c = 0; c < kDirectMaxBuildPayload; ++c) bv[c][j] = 0;
       if (!(hit >> j & 1u)) continue;
-      const int64_t r = r0 + 32 * j;
+      const uint32_t r = r0 + 32 * j;
       if (a.out_prid) prid[j] = a.prid_map ? __ldcs(a.prid_map + r) : (int32_t)r;
 #pragma unroll
       for (int c = 0; c < kDirectMaxProbePayload; ++c)
         if (c < n_pin) pv[c][j] = ld_cs_w(a.pin[c], r, kFixed ? 8 : a.pin_w[c]);
       if (use_rec) {
         uint32_t w[8];
-        load_rec(static_cast<const char*>(a.rec) + (int64_t)pos[j] * rec_stride, rec_stride, w);
+        load_rec(static_cast<const char*>(a.rec) + (size_t)(uint32_t)pos[j] * rec_stride, rec_stride, w);
         brid[j] = (int32_t)w[0];
 #pragma unroll
         for (int c = 0; c < kDirectMaxBuildPayload; ++c)
@@ -199,7 +198,7 @@ __global__ void __launch_bounds__(kDirectThreads, (R <= 2 ? 4 : 2))
         const unsigned tot = __shfl_sync(kFullMask, incl, kDirectWarps - 1);
         unsigned long long cb = 0;
         if (lane == 0 && tot) cb = atomicAdd(a.d_count, (unsigned long long)tot);
-        if (lane == 1) s_next = 2 * (int64_t)gridDim.x + (int64_t)atomicAdd(a.tile_ctr, 1ull);
+        if (lane == 1) s_next = 2 * gridDim.x + (uint32_t)atomicAdd(a.tile_ctr, 1ull);
         cb = __shfl_sync(kFullMask, cb, 0);
         if (lane < kDirectWarps) s_wbase[lane] = cb + (incl - v);
       }
@@ -213,19 +212,19 @@ __global__ void __launch_bounds__(kDirectThreads, (R <= 2 ? 4 : 2))
     tile = nxt;
     nxt = CTA_AGG ? s_next : nxt + gridDim.x;
     if (wtot == 0) continue;
-    int64_t p[R];
+    uint32_t p[R];
     {
-      unsigned run = 0;
+      uint32_t run = (uint32_t)base;
 #pragma unroll
       for (int j = 0; j < R; ++j) {
-        p[j] = (int64_t)(base + run + __popc(bal[j] & below));
+        p[j] = run + __popc(bal[j] & below);
         run += __popc(bal[j]);
       }
     }
     // ---- stores: each row group j is one contiguous run of positions per column ----
 #pragma unroll
     for (int j = 0; j < R; ++j) {
-      if (!(hit >> j & 1u) || p[j] >= a.capacity) continue;
+      if (!(hit >> j & 1u) || p[j] >= cap) continue;
       if (a.out_prid) __stcs(a.out_prid + p[j], prid[j]);
       if (a.out_brid) __stcs(a.out_brid + p[j], brid[j]);
 #pragma unroll
@@ -357,17 +356,13 @@ __global__ void __launch_bounds__(kDirectThreads, 4)
 #pragma unroll
       for (int j = 0; j < R; ++j) {
         if (!(act >> j & 1u)) continue;
-        bool done = false;
-#pragma unroll
-        for (int q = 0; q < Ops::kSlots; ++q) {
-          if (!done && Ops::match_s(bk[j], q, ks[j], kmask)) {
-            pos[j] = Ops::rid(bk[j], q, t.rbits);
-            hit |= 1u << j;
-            done = true;
-          }
-          done |= Ops::empty(bk[j], q);
+        int32_t pj;
+        const bool m = Ops::match_distinct(bk[j], ks[j], kmask, t.rbits, pj);
+        if (m) {
+          pos[j] = pj;
+          hit |= 1u << j;
         }
-        if (done) act &= ~(1u << j);
+        if (m || Ops::open(bk[j])) act &= ~(1u << j);
         else b[j] = next_bucket(b[j], t.segmask);
       }
     }

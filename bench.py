@@ -265,7 +265,7 @@ def run_sj(args):
         ev0.record()
         tb = J.HashTable(bk, attach=bp, partition_bits=args.partition_bits, aggregation=args.aggregation,
                          probe_kernel=args.probe_kernel, rows_per_lane=args.rows_per_lane,
-                         ctas_per_sm=args.ctas_per_sm)
+                         ctas_per_sm=args.ctas_per_sm, load_factor=args.load_factor or 0.5)
         ev1.record()
         torch.cuda.synchronize()
         t_build.append(ev0.elapsed_time(ev1))

@@ -233,7 +233,7 @@ __global__ void __launch_bounds__(kPartThreads) part_scatter_kernel(PartSrc s, i
 constexpr int kFastMaxPay = 2;
 
 struct FastSmem {
-  size_t cur, tcnt, toff, key, rid, part, pay[kFastMaxPay], total;
+  size_t cur, tcnt, toff, key, rid, dst, pay[kFastMaxPay], total;
 };
 
 static FastSmem fast_smem(int pbits, int kw, int n_pay) {
@@ -250,7 +250,7 @@ static FastSmem fast_smem(int pbits, int kw, int n_pay) {
   m.toff = take(P * 4);
   m.key = take((size_t)kTile * kw);
   m.rid = take((size_t)kTile * 4);
-  m.part = take((size_t)kTile * 2);
+  m.dst = take((size_t)kTile * 4);
   for (int c = 0; c < n_pay; ++c) m.pay[c] = take((size_t)kTile * 8);
   m.total = o;
   return m;
@@ -297,7 +297,7 @@ __global__ void __launch_bounds__(kPartThreads, 3) part_scatter_fast_kernel(Part
   unsigned int* toff = reinterpret_cast<unsigned int*>(sm + m.toff);
   K* skey = reinterpret_cast<K*>(sm + m.key);
   int32_t* srid = reinterpret_cast<int32_t*>(sm + m.rid);
-  uint16_t* spart = reinterpret_cast<uint16_t*>(sm + m.part);
+  uint32_t* sdst = reinterpret_cast<uint32_t*>(sm + m.dst);
   __shared__ unsigned int s_wsum[kPartThreads / 32];
   const int P = 1 << pbits;
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
@@ -355,14 +355,15 @@ __global__ void __launch_bounds__(kPartThreads, 3) part_scatter_fast_kernel(Part
     unsigned tile_valid = 0;
     for (int w = 0; w < kPartThreads / 32; ++w) tile_valid += s_wsum[w];
     __syncthreads();
-    // 3. counting-sort the tile into shared memory (payloads straight to their sorted slot)
+    // 3. counting-sort the tile into shared memory (payloads straight to their sorted slot, with
+    //    each row's output position, so the write-out reads nothing per partition)
 #pragma unroll
     for (int j = 0; j < kTileRowsPerThread; ++j) {
       if (pr[j] < 0) continue;
       const unsigned slot = toff[pr[j]] + rank[j];
       skey[slot] = kk[j];
       srid[slot] = (int32_t)(t0 + j * kPartThreads + tid);
-      spart[slot] = (uint16_t)pr[j];
+      sdst[slot] = (uint32_t)cur[pr[j]] + rank[j];
 #pragma unroll
       for (int c = 0; c < NP; ++c) reinterpret_cast<uint64_t*>(sm + m.pay[c])[slot] = pv[c][j];
     }
@@ -370,8 +371,7 @@ __global__ void __launch_bounds__(kPartThreads, 3) part_scatter_fast_kernel(Part
     // 4. loads of the next tile go out before this tile's write-out
     if (t0 + kTile < hi) fast_load_tile<K, NP>(s, t0 + kTile, hi, kk, pv, live);
     for (unsigned slot = tid; slot < tile_valid; slot += kPartThreads) {
-      const int p = spart[slot];
-      const int64_t pos = (int64_t)cur[p] + (slot - toff[p]);
+      const uint32_t pos = sdst[slot];
       okeys[pos] = skey[slot];
       d.rid[pos] = srid[slot];
 #pragma unroll

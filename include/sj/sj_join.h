@@ -128,7 +128,14 @@ typedef enum sj_slot_kind {
 /* Output reservation of the single-pass probe: matches are always compacted warp-aggregated
  * (prefix over the lanes' hit counts); the range is then reserved with one atomicAdd per warp or
  * one per CTA tile. AUTO picks per-CTA for probes of 2^20 rows or more. */
-typedef enum sj_aggregation { SJ_AGG_AUTO = 0, SJ_AGG_WARP = 1, SJ_AGG_CTA = 2 } sj_aggregation;
+/* How probe matches reserve output positions: one atomicAdd per warp, per CTA tile (for probes of
+ * 2^20 rows or more under AUTO), or per warp with warps taking tiles from a shared counter. */
+typedef enum sj_aggregation {
+  SJ_AGG_AUTO = 0,
+  SJ_AGG_WARP = 1,
+  SJ_AGG_CTA = 2,
+  SJ_AGG_WARP_DYNAMIC = 3
+} sj_aggregation;
 
 /* Tunables. Zero-initialised fields take defaults (sj_default_params fills them in). */
 /* How a DISTINCT probe reads its rows and writes its output. DIRECT: lanes write their own

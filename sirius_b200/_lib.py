@@ -21,7 +21,7 @@ SJ_INT8, SJ_INT16, SJ_INT32, SJ_INT64, SJ_FLOAT32, SJ_FLOAT64, SJ_BOOL8, SJ_UINT
 SJ_LAYOUT_AUTO, SJ_LAYOUT_DISTINCT, SJ_LAYOUT_GROUPED = 0, 1, 2
 SJ_NULLS_UNEQUAL, SJ_NULLS_EQUAL = 0, 1
 SJ_SLOT_PACKED64, SJ_SLOT_WIDE128 = 0, 1
-SJ_AGG_AUTO, SJ_AGG_WARP, SJ_AGG_CTA = 0, 1, 2
+SJ_AGG_AUTO, SJ_AGG_WARP, SJ_AGG_CTA, SJ_AGG_WARP_DYNAMIC = 0, 1, 2, 3
 SJ_JOIN_INNER, SJ_JOIN_LEFT, SJ_JOIN_SEMI, SJ_JOIN_ANTI, SJ_JOIN_MARK, SJ_JOIN_FULL = range(6)
 SJ_NO_ROW = -(1 << 31)
 SJ_PROBE_KERNEL_AUTO, SJ_PROBE_KERNEL_STAGED, SJ_PROBE_KERNEL_DIRECT, SJ_PROBE_KERNEL_DIRECT_TMA = 0, 1, 2, 3

@@ -60,7 +60,10 @@ __device__ __forceinline__ void load_rec(const void* p, int stride, uint32_t (&w
 
 // SP / SB >= 0: a compile-time output shape (SP probe payloads, SB attached build fields from the
 // row store, every width 8 bytes); -1: the shape is read from `a` at run time.
-template <typename K, bool WIDE, int R, bool CTA_AGG, int SP = -1, int SB = -1>
+// AGG: 0 = one output atomicAdd per warp, static grid-stride CTA tiles; 1 = one per CTA tile (2 CTA
+// barriers), CTA tiles from the shared counter; 2 = one per warp, warp tiles from the shared counter
+// (no barriers).
+template <typename K, bool WIDE, int R, int AGG, int SP = -1, int SB = -1>
 __global__ void __launch_bounds__(kDirectThreads, (R <= 2 ? 4 : 2))
     probe_direct_kernel(TableDev t, const K* __restrict__ keys, const uint32_t* __restrict__ kv, int64_t kvoff,
                         int64_t n_host, const int64_t* d_n, DirectArgs a) {
@@ -79,21 +82,25 @@ __global__ void __launch_bounds__(kDirectThreads, (R <= 2 ? 4 : 2))
   // probe never has more matches than rows
   const uint32_t n = (uint32_t)(d_n ? *d_n : n_host);
   const uint32_t cap = (uint32_t)(a.capacity < (int64_t)n ? a.capacity : (int64_t)n);
-  constexpr uint32_t kRowsCta = (uint32_t)kDirectThreads * R;
+  constexpr bool CTA_AGG = AGG == 1;
+  constexpr bool kWarpTiles = AGG == 2;
+  constexpr uint32_t kRowsCta = kWarpTiles ? 32u * R : (uint32_t)kDirectThreads * R;  // rows per tile
   const uint32_t tiles = (n + kRowsCta - 1) / kRowsCta;
+  const uint32_t units = kWarpTiles ? gridDim.x * kDirectWarps : gridDim.x;  // tile takers
   const uint64_t kmask = ~((1ull << t.rbits) - 1);
-  const uint32_t lane_off = (uint32_t)warp * (32 * R) + lane;  // row of group j: tile start + lane_off + 32 j
+  const uint32_t lane_off = kWarpTiles ? (uint32_t)lane : (uint32_t)warp * (32 * R) + lane;  // + 32 j
+  const uint32_t first = kWarpTiles ? blockIdx.x * kDirectWarps + warp : blockIdx.x;
   __shared__ uint32_t s_next;
   K k[R];
 #pragma unroll
   for (int j = 0; j < R; ++j) {
-    const uint32_t r = blockIdx.x * kRowsCta + lane_off + 32 * j;
+    const uint32_t r = first * kRowsCta + lane_off + 32 * j;
     k[j] = r < n ? __ldcs(keys + r) : (K)0;
   }
   // Tiles: the first two of a CTA are static (blockIdx.x, + gridDim.x); with CTA reservation the
   // later ones come from a shared tile counter, so the CTAs sweep the (partition-ordered) probe
   // rows together and the table rows in use stay one partition's worth, resident in L2.
-  uint32_t tile = blockIdx.x, nxt = tile + gridDim.x;
+  uint32_t tile = first, nxt = tile + units;
   while (tile < tiles) {
     const uint32_t r0 = tile * kRowsCta + lane_off;
     uint32_t act = 0;
@@ -184,6 +191,7 @@ __global__ void __launch_bounds__(kDirectThreads, (R <= 2 ? 4 : 2))
       wtot += __popc(bal[j]);
     }
     unsigned long long base;
+    uint32_t nn = 0;  // AGG 2: this warp's next tile
     if (CTA_AGG) {
       if (lane == 0) s_wtot[warp] = wtot;
       __syncthreads();
@@ -207,10 +215,12 @@ __global__ void __launch_bounds__(kDirectThreads, (R <= 2 ? 4 : 2))
     } else {
       base = 0;
       if (lane == 0 && wtot) base = atomicAdd(a.d_count, (unsigned long long)wtot);
+      if (kWarpTiles && lane == 1) nn = 2 * units + (uint32_t)atomicAdd(a.tile_ctr, 1ull);
       base = __shfl_sync(kFullMask, base, 0);
+      if (kWarpTiles) nn = __shfl_sync(kFullMask, nn, 1);
     }
     tile = nxt;
-    nxt = CTA_AGG ? s_next : nxt + gridDim.x;
+    nxt = CTA_AGG ? s_next : kWarpTiles ? nn : nxt + units;
     if (wtot == 0) continue;
     uint32_t p[R];
     {
@@ -521,7 +531,7 @@ static void fixed_shape(const DirectArgs& a, int& sp, int& sb) {
   sb = a.n_bin;
 }
 
-template <typename K, bool WIDE, int R, bool CTA, int SP, int SB>
+template <typename K, bool WIDE, int R, int CTA, int SP, int SB>
 static void launch_direct_shape(const sj_table* t, const sj_column& p, const int64_t* d_n, const DirectArgs& a,
                                 cudaStream_t s) {
   int resident = 0;
@@ -534,7 +544,7 @@ static void launch_direct_shape(const sj_table* t, const sj_column& p, const int
       table_dev(t), static_cast<const K*>(p.data), p.validity, p.validity_offset, p.num_rows, d_n, a);
 }
 
-template <typename K, bool WIDE, int R, bool CTA>
+template <typename K, bool WIDE, int R, int CTA>
 static void launch_direct_kernel(const sj_table* t, const sj_column& p, const int64_t* d_n, const DirectArgs& a,
                                  cudaStream_t s) {
   int sp, sb;
@@ -548,13 +558,14 @@ static void launch_direct_kernel(const sj_table* t, const sj_column& p, const in
 
 template <typename K, bool WIDE>
 static void launch_direct(const sj_table* t, const sj_column& p, const int64_t* d_n, const DirectArgs& a, int rpl,
-                          bool cta, cudaStream_t s) {
+                          int mode, cudaStream_t s) {
   if (rpl >= 4) {
-    if (cta) launch_direct_kernel<K, WIDE, 4, true>(t, p, d_n, a, s);
-    else launch_direct_kernel<K, WIDE, 4, false>(t, p, d_n, a, s);
+    if (mode == 1) launch_direct_kernel<K, WIDE, 4, 1>(t, p, d_n, a, s);
+    else launch_direct_kernel<K, WIDE, 4, 0>(t, p, d_n, a, s);
   } else {
-    if (cta) launch_direct_kernel<K, WIDE, 2, true>(t, p, d_n, a, s);
-    else launch_direct_kernel<K, WIDE, 2, false>(t, p, d_n, a, s);
+    if (mode == 1) launch_direct_kernel<K, WIDE, 2, 1>(t, p, d_n, a, s);
+    else if (mode == 2) launch_direct_kernel<K, WIDE, 2, 2>(t, p, d_n, a, s);
+    else launch_direct_kernel<K, WIDE, 2, 0>(t, p, d_n, a, s);
   }
 }
 
@@ -602,16 +613,17 @@ bool probe_direct(const sj_table* t, const sj_column& p, const int64_t* d_n, con
     return true;
   }
   const int agg = pr.aggregation;
-  const bool cta = agg == SJ_AGG_CTA || (agg == SJ_AGG_AUTO && p.num_rows >= (1 << 20));
+  const int mode = agg == SJ_AGG_CTA ? 1 : agg == SJ_AGG_WARP_DYNAMIC ? 2 : agg == SJ_AGG_WARP ? 0
+                 : p.num_rows >= (1 << 20) ? 1 : 0;
   const int rpl = pr.rows_per_lane > 0 ? pr.rows_per_lane : 2;
   const bool wide = t->slot_kind == SJ_SLOT_WIDE128;
   KernelTimer timer("probe_direct", s);
   if (t->key_type == SJ_INT32) {
-    if (wide) launch_direct<int32_t, true>(t, p, d_n, a, rpl, cta, s);
-    else launch_direct<int32_t, false>(t, p, d_n, a, rpl, cta, s);
+    if (wide) launch_direct<int32_t, true>(t, p, d_n, a, rpl, mode, s);
+    else launch_direct<int32_t, false>(t, p, d_n, a, rpl, mode, s);
   } else {
-    if (wide) launch_direct<int64_t, true>(t, p, d_n, a, rpl, cta, s);
-    else launch_direct<int64_t, false>(t, p, d_n, a, rpl, cta, s);
+    if (wide) launch_direct<int64_t, true>(t, p, d_n, a, rpl, mode, s);
+    else launch_direct<int64_t, false>(t, p, d_n, a, rpl, mode, s);
   }
   return true;
 }

@@ -61,6 +61,14 @@ def test_kernels_match_oracle(cuda, kernel, dtype, pbits, attach):
     assert_same_rows(got, oracle_join(inp))
 
 
+@pytest.mark.parametrize("agg", [L.SJ_AGG_WARP, L.SJ_AGG_CTA, L.SJ_AGG_WARP_DYNAMIC])
+def test_direct_output_reservation_modes(cuda, agg):
+    inp = _input(15, np.int64, 300_001, 2_000_003)
+    for pbits in (-1, 3):
+        got = _run(inp, cuda, L.SJ_PROBE_KERNEL_DIRECT, True, partition_bits=pbits, aggregation=agg)
+        assert_same_rows(got, oracle_join(inp))
+
+
 @pytest.mark.parametrize("kernel", KERNELS)
 def test_kernels_wide_slots_and_null_probe_keys(cuda, kernel):
     inp = _input(12, np.int64, 150_001, 700_001, null_frac=0.05, full_range=True)

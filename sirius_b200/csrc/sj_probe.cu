@@ -483,18 +483,37 @@ __global__ void __launch_bounds__(kExpandThreads) expand_kernel(const int32_t* _
       s_start[i] = m_start[e0 + i];
     }
     __syncthreads();
-    // 1. entries (shared memory only)
+    // 1. entries (shared memory only). Warp w covers positions j0 + m*256 + 32w + lane, 32
+    //    consecutive outputs per m. Lane m finds the entry of the warp's first position for item m
+    //    (binary search); the entries of the 32 lanes are then that entry plus the number of entry
+    //    starts at or below each lane: the next 31 starts are loaded one per lane and their lane
+    //    offsets OR-ed into a mask, so a lane's entry is one popc away.
     int32_t row[kExpandItems], gi[kExpandItems];
-    int e = 0;
+    {
+      const int warp = threadIdx.x >> 5;
+      const int64_t jw0 = j0 + 32 * warp;  // warp's first position for m = 0
+      int eb = 0;
+      if (lane < kExpandItems) {
+        const int64_t jb = jw0 + (int64_t)lane * kExpandThreads;
+        eb = jb < j1 ? (int)upper_index(s_off, 0, ne - 1, jb) : 0;
+      }
 #pragma unroll
-    for (int m = 0; m < kExpandItems; ++m) {
-      const int64_t j = j0 + (int64_t)m * kExpandThreads + threadIdx.x;
-      row[m] = 0;
-      gi[m] = -1;
-      if (j < j1) {
-        e = m == 0 ? (int)upper_index(s_off, 0, ne - 1, j) : gallop_index(s_off, e, ne - 1, j);
-        row[m] = s_row[e];
-        gi[m] = s_start[e] + (int32_t)(j - s_off[e]);
+      for (int m = 0; m < kExpandItems; ++m) {
+        const int64_t jb = jw0 + (int64_t)m * kExpandThreads;
+        const int e_base = __shfl_sync(kFullMask, eb, m);
+        const int64_t j = jb + lane;
+        row[m] = 0;
+        gi[m] = -1;
+        if (jb >= j1) continue;  // warp-uniform
+        const int nb = e_base + 1 + lane;
+        const int64_t rel = (lane < 31 && nb < ne) ? s_off[nb] - jb : 64;
+        const unsigned starts = __reduce_or_sync(kFullMask, rel < 32 ? (1u << rel) : 0u);
+        const unsigned upto = lane == 31 ? kFullMask : ((2u << lane) - 1u);
+        const int e = e_base + __popc(starts & upto);
+        if (j < j1) {
+          row[m] = s_row[e];
+          gi[m] = s_start[e] + (int32_t)(j - s_off[e]);
+        }
       }
     }
     // 2. group members (table positions)
@@ -745,12 +764,13 @@ static size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
 // the table's partition bits, then stream the partitioned arrays through the probe kernel, so
 // each partition's probes hit its L2-resident table segment and attached payload rows.
 // Probe-side radix bits: the coarsest prefix of the table's partition bits whose share of the
-// table footprint (slots + position map + attached payloads) stays under ~40 MB of L2. A coarse
+// table footprint (slots + position map + attached payloads) stays under 48 MB of L2. A coarse
 // probe partition covers 2^(table bits - probe bits) contiguous table segments, and fewer
-// partitions mean longer contiguous runs in the scatter.
+// partitions mean longer contiguous runs in the scatter (16M-row table, 768 MB: 12 MB shares made
+// the probe 2 % faster and the scatter 15 % slower than 48 MB shares; 24 MB was in between).
 static int probe_partition_bits(const sj_table* t) {
   size_t fp = t->slots_bytes + t->arow_bytes;
-  const size_t kShare = 40ull << 20;
+  const size_t kShare = 48ull << 20;
   int b = 1;
   while (b < t->pbits && (fp >> b) > kShare) ++b;
   return std::min(b, t->pbits);

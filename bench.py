@@ -48,8 +48,8 @@ def parse():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="sj", choices=["sj", "reference"])
-    ap.add_argument("--n-build", type=int, default=16 << 20)
-    ap.add_argument("--n-probe", type=int, default=64 << 20)
+    ap.add_argument("--n-build", type=int, default=None, help="build rows (default: the workload's)")
+    ap.add_argument("--n-probe", type=int, default=None, help="probe rows (default: the workload's)")
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--cpu-steps", type=int, default=2)
@@ -683,7 +683,8 @@ def run_other(args):
     from sirius_b200 import _lib
     torch.cuda.set_device(0)
     dev = torch.device("cuda", 0)
-    inp = D.small(args.seed) if args.workload == "small" else D.skewed(args.seed)
+    sizes = {k: v for k, v in (("n_build", args.n_build), ("n_probe", args.n_probe)) if v}
+    inp = D.small(args.seed, **sizes) if args.workload == "small" else D.skewed(args.seed, **sizes)
     bk = torch.from_numpy(inp.build_keys).to(dev)
     pk = torch.from_numpy(inp.probe_keys).to(dev)
     pv = None if inp.probe_validity is None else torch.from_numpy(inp.probe_validity.view(np.int32)).to(dev)
@@ -762,10 +763,10 @@ def run_other(args):
             assert r.rows == m
         cpu = {"value": round(inp.n_probe / statistics.median(ts) / 1e6, 3), "unit": "Mtuples/s", "cores": threads,
                "kind": "port", "sample": f"full workload, {len(ts)} one-shot CPU joins, median {statistics.median(ts):.3f} s"}
-    desc = ("small: build 100,000 unique int32 keys (permutation) + int32 payload; probe 1,000,000 int32 keys "
-            "uniform over 0..109,999 + int32 payload" if args.workload == "small" else
-            "skewed: build 8M int64 keys Zipf(1.1) over 1M values + int32 payload; probe 32M int64 keys Zipf(0.8) "
-            "over 2M values (half absent), 5% NULL")
+    desc = (f"small: build {inp.n_build} unique int32 keys (permutation) + int32 payload; probe {inp.n_probe} "
+            f"int32 keys uniform over 1.1x the build range + int32 payload" if args.workload == "small" else
+            f"skewed: build {inp.n_build} int64 keys Zipf(1.1) over 1M values + int32 payload; probe {inp.n_probe} "
+            f"int64 keys Zipf(0.8) over 2M values (half absent), 5% NULL")
     line = {
         "metric": "join probe Mtuples/s", "value": round(inp.n_probe / (ms / 1e3) / 1e6, 3), "unit": "Mtuples/s",
         "n_gpus": 1, "steps": args.steps, "warmup": max(3, args.warmup), "ms_per_step": round(ms, 4),
@@ -787,6 +788,9 @@ def run_other(args):
 
 def main():
     args = parse()
+    if args.workload == "large" or args.impl == "reference":
+        args.n_build = args.n_build or 16 << 20
+        args.n_probe = args.n_probe or 64 << 20
     if args.impl == "reference":
         return run_reference(args)
     if args.workload == "batched":

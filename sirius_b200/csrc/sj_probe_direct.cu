@@ -25,7 +25,7 @@ namespace sj {
 
 TableDev table_dev(const sj_table* t);
 
-constexpr int kDirectThreads = 256;
+constexpr int kDirectThreads = 64;  // 2 warps: the reservation barriers wait on one other warp only
 constexpr int kDirectWarps = kDirectThreads / 32;
 
 __device__ __forceinline__ uint64_t ld_cs_w(const void* base, int64_t i, int w) {
@@ -64,7 +64,7 @@ __device__ __forceinline__ void load_rec(const void* p, int stride, uint32_t (&w
 // barriers), CTA tiles from the shared counter; 2 = one per warp, warp tiles from the shared counter
 // (no barriers).
 template <typename K, bool WIDE, int R, int AGG, int SP = -1, int SB = -1>
-__global__ void __launch_bounds__(kDirectThreads, (R <= 2 ? 4 : 2))
+__global__ void __launch_bounds__(kDirectThreads, (R <= 2 ? 1024 : 512) / kDirectThreads)
     probe_direct_kernel(TableDev t, const K* __restrict__ keys, const uint32_t* __restrict__ kv, int64_t kvoff,
                         int64_t n_host, const int64_t* d_n, DirectArgs a) {
   using Ops = SlotOps<WIDE>;
@@ -538,7 +538,8 @@ static void launch_direct_shape(const sj_table* t, const sj_column& p, const int
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, probe_direct_kernel<K, WIDE, R, CTA, SP, SB>,
                                                 kDirectThreads, 0);
   const int64_t tiles = (p.num_rows + (int64_t)kDirectThreads * R - 1) / ((int64_t)kDirectThreads * R);
-  const int per_sm = std::min(std::max(1, resident), std::max(1, t->params.ctas_per_sm));
+  // ctas_per_sm counts 256-thread CTAs
+  const int per_sm = std::min(std::max(1, resident), std::max(1, t->params.ctas_per_sm) * 256 / kDirectThreads);
   const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(tiles, (int64_t)sm_count(t->device) * per_sm));
   probe_direct_kernel<K, WIDE, R, CTA, SP, SB><<<grid, kDirectThreads, 0, s>>>(
       table_dev(t), static_cast<const K*>(p.data), p.validity, p.validity_offset, p.num_rows, d_n, a);

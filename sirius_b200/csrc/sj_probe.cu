@@ -815,7 +815,7 @@ static sj_status probe_partitioned(const sj_table* t, const sj_column& p, Gather
   for (int c = 0; c < g.n_pin; ++c)
     g.pin[c] = PayloadIn{pd.pay[c], nullptr, pd.valid8[c], 0, g.pin[c].width, g.pin[c].width, 1, 0};
   const sj_column pk{pd.keys, nullptr, 0, n, t->key_type, 0};
-  if (!probe_direct(t, pk, d_total, g, s, tile_ctr)) dispatch_distinct<false>(t, pk, d_total, g, s);
+  if (!probe_direct(t, pk, d_total, g, s, alloc, tile_ctr)) dispatch_distinct<false>(t, pk, d_total, g, s);
   SJ_CUDA_TRY(cudaGetLastError());
   return SJ_OK;
 }
@@ -838,9 +838,7 @@ sj_status probe_gather(const sj_table* t, const sj_column& p, const GatherSpec& 
 
   if (t->layout == SJ_LAYOUT_DISTINCT) {
     if (t->pbits > 0 && p.num_rows >= kMinPartitionedProbe) return probe_partitioned(t, p, g, alloc, s);
-    Scratch ctr;
-    SJ_TRY(ctr.get(alloc, 256, s));
-    if (!probe_direct(t, p, nullptr, g, s, ctr.as<unsigned long long>())) dispatch_distinct<false>(t, p, nullptr, g, s);
+    if (!probe_direct(t, p, nullptr, g, s, alloc, nullptr)) dispatch_distinct<false>(t, p, nullptr, g, s);
     SJ_CUDA_TRY(cudaGetLastError());
     return SJ_OK;
   }

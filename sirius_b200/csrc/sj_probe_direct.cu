@@ -63,6 +63,19 @@ __device__ __forceinline__ void load_rec(const void* p, int stride, uint32_t (&w
 // AGG: 0 = one output atomicAdd per warp, static grid-stride CTA tiles; 1 = one per CTA tile (2 CTA
 // barriers), CTA tiles from the shared counter; 2 = one per warp, warp tiles from the shared counter
 // (no barriers).
+// Field of `width` (4 or 8) bytes at byte offset `off` of a record held in 8 words, picked with
+// predicated moves so the record stays in registers.
+__device__ __forceinline__ uint64_t rec_word_field(const uint32_t (&w)[8], int off, int width) {
+  const int wi = off >> 2;
+  uint32_t lo = 0, hi = 0;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    lo = k == wi ? w[k] : lo;
+    hi = k == wi + 1 ? w[k] : hi;
+  }
+  return width == 8 ? ((uint64_t)hi << 32) | lo : lo;
+}
+
 template <typename K, bool WIDE, int R, int AGG, int SP = -1, int SB = -1>
 __global__ void __launch_bounds__(kDirectThreads, (R <= 2 ? 1024 : 512) / kDirectThreads)
     probe_direct_kernel(TableDev t, const K* __restrict__ keys, const uint32_t* __restrict__ kv, int64_t kvoff,
@@ -169,7 +182,8 @@ __global__ void __launch_bounds__(kDirectThreads, (R <= 2 ? 1024 : 512) / kDirec
         brid[j] = (int32_t)w[0];
 #pragma unroll
         for (int c = 0; c < kDirectMaxBuildPayload; ++c)
-          bv[c][j] = ((uint64_t)w[3 + 2 * c] << 32) | w[2 + 2 * c];
+          bv[c][j] = kFixed || a.rec_std ? ((uint64_t)w[3 + 2 * c] << 32) | w[2 + 2 * c]
+                                         : rec_word_field(w, a.rec_off[c], a.bin_w[c]);
       } else {
         brid[j] = a.brid_map ? __ldg(reinterpret_cast<const int32_t*>(reinterpret_cast<const char*>(a.brid_map) +
                                                                        (int64_t)pos[j] * a.brid_stride))
@@ -495,15 +509,18 @@ bool direct_args(const GatherArgs& g, DirectArgs& a) {
     a.pout[c] = g.pout[c].data;
   }
   if (g.n_bin > 0 && g.rec) {
-    if (g.rec_stride != 16 && g.rec_stride != 32) return false;
-    for (int c = 0; c < g.n_bin; ++c)
-      if (g.bin[c].width != 8 || g.rec_voff[c] >= 0 || g.rec_off[c] != 8 + 8 * c) return false;
-    a.rec = g.rec;
-    a.rec_stride = g.rec_stride;
+    if (g.rec_stride != 8 && g.rec_stride != 16 && g.rec_stride != 32) return false;
+    a.rec_std = 1;
     for (int c = 0; c < g.n_bin; ++c) {
-      a.bin_w[c] = 8;
+      const int w = g.bin[c].width;
+      if ((w != 4 && w != 8) || g.rec_voff[c] >= 0) return false;
+      if (w != 8 || g.rec_off[c] != 8 + 8 * c) a.rec_std = 0;
+      a.rec_off[c] = g.rec_off[c];
+      a.bin_w[c] = w;
       a.bout[c] = g.bout[c].data;
     }
+    a.rec = g.rec;
+    a.rec_stride = g.rec_stride;
     return true;
   }
   a.brid_map = g.brid_map;
@@ -525,7 +542,7 @@ static void fixed_shape(const DirectArgs& a, int& sp, int& sb) {
   sp = sb = -1;
   for (int c = 0; c < a.n_pin; ++c)
     if (a.pin_w[c] != 8) return;
-  if (a.n_bin > 0 && (!a.rec || a.rec_stride != (a.n_bin == 1 ? 16 : 32))) return;
+  if (a.n_bin > 0 && (!a.rec || !a.rec_std || a.rec_stride != (a.n_bin == 1 ? 16 : 32))) return;
   if (a.n_bin == 0 && a.rec) return;
   sp = a.n_pin;
   sb = a.n_bin;
@@ -589,16 +606,26 @@ static void launch_tma(const sj_table* t, const sj_column& p, const int64_t* d_n
 }
 
 bool probe_direct(const sj_table* t, const sj_column& p, const int64_t* d_n, const GatherArgs& g, cudaStream_t s,
-                  unsigned long long* tile_ctr) {
+                  const Allocator& alloc, unsigned long long* tile_ctr) {
   const sj_join_params& pr = t->params;
   if (pr.probe_kernel == SJ_PROBE_KERNEL_STAGED) return false;
   DirectArgs a;
   if (!direct_args(g, a)) return false;
-  if (cudaMemsetAsync(tile_ctr, 0, sizeof(unsigned long long), s) != cudaSuccess) return false;
+  const int agg = pr.aggregation;
+  const int mode = agg == SJ_AGG_CTA ? 1 : agg == SJ_AGG_WARP_DYNAMIC ? 2 : agg == SJ_AGG_WARP ? 0
+                 : p.num_rows >= (1 << 20) ? 1 : 0;
+  Scratch ctr;  // released (stream-ordered) after the launch below
+  if (mode != 0 || pr.probe_kernel == SJ_PROBE_KERNEL_DIRECT_TMA) {
+    if (!tile_ctr) {
+      if (ctr.get(alloc, 256, s) != SJ_OK) return false;
+      tile_ctr = ctr.as<unsigned long long>();
+    }
+    if (cudaMemsetAsync(tile_ctr, 0, sizeof(unsigned long long), s) != cudaSuccess) return false;
+  }
   a.tile_ctr = tile_ctr;
   // AUTO takes the plain-load kernel: on the large 1:1 join the TMA ring's per-tile CTA barriers
   // cost more than the DRAM latency it hides (measured 1.96 vs 1.73 ms per 64M probe rows)
-  bool tma = pr.probe_kernel == SJ_PROBE_KERNEL_DIRECT_TMA;
+  bool tma = pr.probe_kernel == SJ_PROBE_KERNEL_DIRECT_TMA && (!a.rec || a.rec_std);
   tma = tma && al16(p.data) && (!a.prid_map || al16(a.prid_map));
   for (int c = 0; c < a.n_pin; ++c) tma = tma && al16(a.pin[c]);
   if (tma) {
@@ -613,9 +640,6 @@ bool probe_direct(const sj_table* t, const sj_column& p, const int64_t* d_n, con
     }
     return true;
   }
-  const int agg = pr.aggregation;
-  const int mode = agg == SJ_AGG_CTA ? 1 : agg == SJ_AGG_WARP_DYNAMIC ? 2 : agg == SJ_AGG_WARP ? 0
-                 : p.num_rows >= (1 << 20) ? 1 : 0;
   const int rpl = pr.rows_per_lane > 0 ? pr.rows_per_lane : 2;
   const bool wide = t->slot_kind == SJ_SLOT_WIDE128;
   KernelTimer timer("probe_direct", s);

@@ -16,8 +16,10 @@ struct DirectArgs {
   const int32_t* brid_map;  // table position -> build row id at brid_map + pos * brid_stride bytes
   int32_t brid_stride;
   int32_t bin_by_pos;       // build payload element index: table position (1) or build row id (0)
-  const void* rec;          // row store (record = [row id | pad | 8-byte fields]) or NULL
+  const void* rec;          // row store (record = [row id | fields]) or NULL
   int32_t rec_stride;
+  int32_t rec_std;          // fields are 8-byte at offsets 8, 16, 24 (else rec_off / bin_w)
+  int16_t rec_off[kDirectMaxBuildPayload];
   int32_t n_pin, n_bin;
   const void* pin[kDirectMaxProbePayload];
   int32_t pin_w[kDirectMaxProbePayload];
@@ -37,8 +39,9 @@ bool direct_args(const GatherArgs& g, DirectArgs& a);
 
 // Launches the direct probe of DISTINCT table `t` when the shape allows and the table's
 // parameters do not ask for the staged kernel; returns false (nothing launched) otherwise.
-// `tile_ctr`: a device word the launch may use as its tile counter (zeroed here, on `s`).
+// `tile_ctr`: a device word the launch may use as its tile counter (zeroed here, on `s`); when NULL
+// and a counter is needed, one is drawn from `alloc`.
 bool probe_direct(const sj_table* t, const sj_column& p, const int64_t* d_n, const GatherArgs& g, cudaStream_t s,
-                  unsigned long long* tile_ctr);
+                  const Allocator& alloc, unsigned long long* tile_ctr);
 
 }  // namespace sj

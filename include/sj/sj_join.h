@@ -197,9 +197,14 @@ SJ_EXPORT void sj_default_params(sj_join_params* params);
 
 /* Build a hash table over the build keys (replaces the cudf::hash_join / distinct_hash_join
  * constructors, src/op/sirius_physical_hash_join.cpp:1614-1620). Row ids in the table are the
- * build column's row indices. Only num_keys == 1 is accepted. Rows with a NULL key are not
- * inserted under SJ_NULLS_UNEQUAL. The key column is only read during the call; the caller keeps
- * the build batch alive for the gather, as the operator does (:1593).
+ * build column's row indices. num_keys 1..4: several INT32/INT64 key columns form a composite key
+ * (the operator's multi-column conditions, prepare_join_keys, :1234-1291), packed exactly into one
+ * 64-bit key from the build's per-column value ranges — refused with SJ_ERR_INVALID when the ranges
+ * need more than 63 bits; every probe of the table then passes the same number of key columns.
+ * Rows with a NULL key (any NULL column) are not inserted under SJ_NULLS_UNEQUAL; under
+ * SJ_NULLS_EQUAL a NULL column compares equal to NULL column by column. The key columns are only
+ * read during the call; the caller keeps the build batch alive for the gather, as the operator
+ * does (:1593).
  * Synchronizes `stream` (once to size the table from the key range, once to choose the layout);
  * the reference synchronizes after the build as well (:1622). */
 SJ_EXPORT sj_status sj_build(const sj_column* keys, int32_t num_keys, const sj_join_params* params,

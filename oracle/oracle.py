@@ -244,6 +244,28 @@ def gather_nullable(col, rid, valid=None):
     return v, m
 
 
+def composite_keys(build_cols, probe_cols, build_valid=None, probe_valid=None, nulls_equal=False):
+    """Equi-join on several key columns reduced to one: each distinct tuple of key values (over both
+    sides) gets an int64 id. Returns (build ids, probe ids, build validity words, probe validity
+    words). NULLs unequal: a row with any NULL key column has a NULL id; NULLs equal: a NULL is one
+    more value of its column (IS NOT DISTINCT FROM on every column)."""
+    nb, npr = len(build_cols[0]), len(probe_cols[0])
+    build_valid = build_valid or [None] * len(build_cols)
+    probe_valid = probe_valid or [None] * len(probe_cols)
+    parts, all_valid = [], np.ones(nb + npr, bool)
+    for bc, pc, bv, pv in zip(build_cols, probe_cols, build_valid, probe_valid):
+        vals = np.concatenate([np.asarray(bc, np.int64), np.asarray(pc, np.int64)])
+        ok = np.concatenate([unpack_validity(bv, nb) if bv is not None else np.ones(nb, bool),
+                             unpack_validity(pv, npr) if pv is not None else np.ones(npr, bool)])
+        parts += [np.where(ok, vals, 0), (~ok).astype(np.int64)]
+        all_valid &= ok
+    _, ids = np.unique(np.stack(parts, axis=1), axis=0, return_inverse=True)
+    ids = ids.reshape(-1).astype(np.int64)
+    if nulls_equal:
+        return ids[:nb], ids[nb:], None, None
+    return ids[:nb], ids[nb:], pack_validity(all_valid[:nb]), pack_validity(all_valid[nb:])
+
+
 # ------------------------------------------------------------------------------------------------
 # Canonical form and order-independent checksum
 # ------------------------------------------------------------------------------------------------

@@ -197,16 +197,29 @@ SJ_EXPORT sj_status sj_build(const sj_column* keys, int32_t num_keys, const sj_j
   clear_error();
   if (!out) return set_error(SJ_ERR_INVALID, "out is NULL");
   *out = nullptr;
-  if (num_keys != 1) return set_error(SJ_ERR_INVALID, "exactly one key column is supported");
-  if (!keys) return set_error(SJ_ERR_INVALID, "keys is NULL");
-  try {
-    const sj_join_params p = resolve(params);
-    return build_table(keys[0], nullptr, 0, p, Allocator(alloc), reinterpret_cast<cudaStream_t>(stream), out);
-  } catch (const std::bad_alloc&) {
-    return set_error(SJ_ERR_OOM, "host allocation failed");
-  } catch (const std::exception& e) {
-    return set_error(SJ_ERR_DEVICE, e.what());
-  }
+  return sj_build_ex(keys, num_keys, nullptr, 0, params, alloc, stream, out);
+}
+
+// Builds on keys[0], or on the packed composite key of 2..4 columns (the table keeps the packing).
+static sj_status build_keys(const sj_column* keys, int32_t num_keys, const sj_column* payload, int32_t num_payload,
+                            const sj_join_params& p, const Allocator& a, cudaStream_t s, sj_table** out) {
+  if (num_keys == 1) return build_table(keys[0], payload, num_payload, p, a, s, out);
+  KeyPack kp{};
+  Scratch buf;
+  sj_column packed{};
+  SJ_TRY(pack_build_keys(keys, num_keys, p.null_equality == SJ_NULLS_EQUAL, a, s, &kp, buf, &packed));
+  SJ_TRY(build_table(packed, payload, num_payload, p, a, s, out));
+  (*out)->kpack = kp;
+  return SJ_OK;
+}
+
+// The probe's key column: keys[0], or the composite key packed as the table's build was.
+static sj_status probe_keys_of(const sj_table* t, const sj_column* keys, int32_t num_keys, const Allocator& a,
+                               cudaStream_t s, Scratch& buf, sj_column* out) {
+  if (t->kpack.n > 1) return pack_probe_keys(t->kpack, keys, num_keys, a, s, buf, out);
+  if (num_keys != 1) return set_error(SJ_ERR_INVALID, "the table was built on one key column");
+  *out = keys[0];
+  return SJ_OK;
 }
 
 SJ_EXPORT sj_status sj_build_ex(const sj_column* keys, int32_t num_keys, const sj_column* payload,
@@ -215,12 +228,12 @@ SJ_EXPORT sj_status sj_build_ex(const sj_column* keys, int32_t num_keys, const s
   clear_error();
   if (!out) return set_error(SJ_ERR_INVALID, "out is NULL");
   *out = nullptr;
-  if (num_keys != 1) return set_error(SJ_ERR_INVALID, "exactly one key column is supported");
+  if (num_keys < 1 || num_keys > kMaxKeyColumns) return set_error(SJ_ERR_INVALID, "1 to 4 key columns");
   if (!keys) return set_error(SJ_ERR_INVALID, "keys is NULL");
   try {
     const sj_join_params p = resolve(params);
-    return build_table(keys[0], payload, num_payload, p, Allocator(alloc), reinterpret_cast<cudaStream_t>(stream),
-                       out);
+    const Allocator a(alloc);
+    return build_keys(keys, num_keys, payload, num_payload, p, a, reinterpret_cast<cudaStream_t>(stream), out);
   } catch (const std::bad_alloc&) {
     return set_error(SJ_ERR_OOM, "host allocation failed");
   } catch (const std::exception& e) {
@@ -261,9 +274,13 @@ SJ_EXPORT sj_status sj_probe_count(const sj_table* table, const sj_column* probe
                                    const sj_alloc* alloc, sj_stream_t stream, int64_t* d_count) {
   clear_error();
   if (!table || !probe_keys || !d_count) return set_error(SJ_ERR_INVALID, "table, probe_keys and d_count are required");
-  if (num_keys != 1) return set_error(SJ_ERR_INVALID, "exactly one key column is supported");
   try {
-    return probe_count(table, probe_keys[0], Allocator(alloc), reinterpret_cast<cudaStream_t>(stream), d_count);
+    const Allocator a(alloc);
+    const cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    Scratch buf;
+    sj_column key{};
+    SJ_TRY(probe_keys_of(table, probe_keys, num_keys, a, s, buf, &key));
+    return probe_count(table, key, a, s, d_count);
   } catch (const std::exception& e) {
     return set_error(SJ_ERR_DEVICE, e.what());
   }
@@ -277,11 +294,15 @@ SJ_EXPORT sj_status sj_probe_gather(const sj_table* table, const sj_column* prob
                                     int64_t capacity, const sj_alloc* alloc, sj_stream_t stream, int64_t* d_count) {
   clear_error();
   if (!table || !probe_keys || !d_count) return set_error(SJ_ERR_INVALID, "table, probe_keys and d_count are required");
-  if (num_keys != 1) return set_error(SJ_ERR_INVALID, "exactly one key column is supported");
   GatherSpec g{probe_payload, num_probe_payload, build_payload, num_build_payload, out_probe_rid,
                out_build_rid, out_probe_payload, out_build_payload, capacity};
   try {
-    return probe_gather(table, probe_keys[0], g, Allocator(alloc), reinterpret_cast<cudaStream_t>(stream), d_count);
+    const Allocator a(alloc);
+    const cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    Scratch buf;
+    sj_column key{};
+    SJ_TRY(probe_keys_of(table, probe_keys, num_keys, a, s, buf, &key));
+    return probe_gather(table, key, g, a, s, d_count);
   } catch (const std::exception& e) {
     return set_error(SJ_ERR_DEVICE, e.what());
   }
@@ -296,12 +317,15 @@ SJ_EXPORT sj_status sj_probe_join(const sj_table* table, sj_join_kind kind, cons
                                   int64_t* d_count) {
   clear_error();
   if (!table || !probe_keys || !d_count) return set_error(SJ_ERR_INVALID, "table, probe_keys and d_count are required");
-  if (num_keys != 1) return set_error(SJ_ERR_INVALID, "exactly one key column is supported");
   GatherSpec g{probe_payload, num_probe_payload, build_payload, num_build_payload, out_probe_rid,
                out_build_rid, out_probe_payload, out_build_payload, capacity};
   try {
-    return probe_join(table, (int32_t)kind, probe_keys[0], g, out_mark, out_mark_validity, Allocator(alloc),
-                      reinterpret_cast<cudaStream_t>(stream), d_count);
+    const Allocator a(alloc);
+    const cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    Scratch buf;
+    sj_column key{};
+    SJ_TRY(probe_keys_of(table, probe_keys, num_keys, a, s, buf, &key));
+    return probe_join(table, (int32_t)kind, key, g, out_mark, out_mark_validity, a, s, d_count);
   } catch (const std::exception& e) {
     return set_error(SJ_ERR_DEVICE, e.what());
   }

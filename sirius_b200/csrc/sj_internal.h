@@ -85,6 +85,20 @@ int type_width(int32_t t);  // bytes per element, 0 if invalid
 // ---- the table -------------------------------------------------------------------------------
 }  // namespace sj
 
+namespace sj {
+constexpr int kMaxKeyColumns = 4;
+// Packing of a composite key (sj_keys.cu): column c's code (key - kmin[c], or null_code[c] for a
+// NULL when NULLs compare equal) at bit shift[c]. n <= 1: a single key column, no packing.
+struct KeyPack {
+  int32_t n;
+  int32_t nulls_equal;
+  int32_t bits_total;
+  int32_t shift[kMaxKeyColumns];
+  int64_t kmin[kMaxKeyColumns];
+  uint64_t null_code[kMaxKeyColumns];  // = max - min + 1 of the build's valid values
+};
+}  // namespace sj
+
 struct sj_table {
   int device = 0;
   sj::Allocator alloc;
@@ -134,6 +148,7 @@ struct sj_table {
   size_t apay_bytes[8] = {};
   size_t apay_valid_bytes[8] = {};
   sj_join_params params{};
+  sj::KeyPack kpack{};  // composite key packing (kpack.n >= 2) or none
   int64_t num_slots() const;
 };
 
@@ -165,6 +180,12 @@ sj_status probe_gather(const sj_table* t, const sj_column& probe, const GatherSp
                        const Allocator& alloc, cudaStream_t stream, int64_t* d_count);
 
 sj_status validate_column(const sj_column* c, const char* what, bool key);
+
+// Composite keys (sj_keys.cu): pack 2..4 key columns into one INT64 column held in `buf`.
+sj_status pack_build_keys(const sj_column* keys, int n_keys, bool nulls_equal, const Allocator& alloc,
+                          cudaStream_t s, KeyPack* kp, Scratch& buf, sj_column* packed);
+sj_status pack_probe_keys(const KeyPack& kp, const sj_column* keys, int n_keys, const Allocator& alloc,
+                          cudaStream_t s, Scratch& buf, sj_column* packed);
 
 // LEFT / SEMI / ANTI / MARK / FULL (sj_probe_kinds.cu); INNER delegates to probe_gather.
 sj_status probe_join(const sj_table* t, int32_t kind, const sj_column& probe, const GatherSpec& g, uint8_t* out_mark,

@@ -60,6 +60,18 @@ def make_column(data: torch.Tensor, validity: Optional[torch.Tensor] = None, val
     return col
 
 
+def _keys(keys, validity=None):
+    """Key argument -> (ctypes column array, number of columns, first tensor). `keys` is a tensor (with
+    `validity`) or a list of tensors / (tensor, validity) pairs: a composite key of 2..4 columns."""
+    if isinstance(keys, (list, tuple)):
+        if validity is not None:
+            raise ValueError("pass (tensor, validity) pairs for composite keys")
+        pairs = [_as_pair(k) for k in keys]
+        cols = [make_column(t, v) for t, v in pairs]
+        return _cols(cols), len(cols), pairs[0][0]
+    return _cols([make_column(keys, validity)]), 1, keys
+
+
 def _cols(cols: Sequence[L.SjColumn], cls=L.SjColumn):
     arr = (cls * max(1, len(cols)))()
     for i, c in enumerate(cols):
@@ -142,18 +154,18 @@ class HashTable:
                                        rows_per_lane=rows_per_lane)
         if ctas_per_sm:
             self.params.ctas_per_sm = ctas_per_sm
-        col = make_column(keys, validity)
+        col, nkeys, first = _keys(keys, validity)
         self.attached = [_as_pair(c) for c in attach]
         if self.attached:
             pay = [make_column(t, v) for t, v in self.attached]
-            st = self._lib.sj_build_ex(ctypes.byref(col), 1, _cols(pay), len(pay), ctypes.byref(self.params), None,
+            st = self._lib.sj_build_ex(col, nkeys, _cols(pay), len(pay), ctypes.byref(self.params), None,
                                        _stream_handle(stream), ctypes.byref(self._handle))
             L.check(st, "sj_build_ex")
         else:
-            st = self._lib.sj_build(ctypes.byref(col), 1, ctypes.byref(self.params), None,
+            st = self._lib.sj_build(col, nkeys, ctypes.byref(self.params), None,
                                     _stream_handle(stream), ctypes.byref(self._handle))
             L.check(st, "sj_build")
-        self.build_rows = keys.numel()
+        self.build_rows = first.numel()
 
     @property
     def handle(self):
@@ -169,9 +181,9 @@ class HashTable:
     def count(self, probe_keys: torch.Tensor, probe_validity: Optional[torch.Tensor] = None,
               stream: Optional[torch.cuda.Stream] = None, d_count: Optional[torch.Tensor] = None) -> torch.Tensor:
         """Device int64[1] holding the number of INNER matches (stream-ordered)."""
-        col = make_column(probe_keys, probe_validity)
-        dc = d_count if d_count is not None else torch.empty(1, dtype=torch.int64, device=probe_keys.device)
-        L.check(self._lib.sj_probe_count(self.handle, ctypes.byref(col), 1, None, _stream_handle(stream),
+        col, nkeys, first = _keys(probe_keys, probe_validity)
+        dc = d_count if d_count is not None else torch.empty(1, dtype=torch.int64, device=first.device)
+        L.check(self._lib.sj_probe_count(self.handle, col, nkeys, None, _stream_handle(stream),
                                          dc.data_ptr()), "sj_probe_count")
         return dc
 
@@ -185,12 +197,13 @@ class HashTable:
         DISTINCT, where the probe row count is an upper bound. With ``sync=False`` the returned
         ``count`` is -1 and the device count stays in ``d_count``.
         """
-        dev = probe_keys.device
+        kcols, nkeys, first = _keys(probe_keys, probe_validity)
+        dev = first.device
         if capacity is None:
             if out is not None:
                 capacity = out.probe_rid.numel() if out.probe_rid is not None else out.probe_payload[0].numel()
             elif self.info().layout == L.SJ_LAYOUT_DISTINCT:
-                capacity = probe_keys.numel()
+                capacity = first.numel()
             else:
                 capacity = int(self.count(probe_keys, probe_validity, stream).item())
         if attached:
@@ -205,9 +218,8 @@ class HashTable:
         pout = [_mut(t, v) for t, v in zip(out.probe_payload, out.probe_payload_validity)]
         bout = [_mut(t, v) for t, v in zip(out.build_payload, out.build_payload_validity)]
         dc = d_count if d_count is not None else torch.empty(1, dtype=torch.int64, device=dev)
-        key = make_column(probe_keys, probe_validity)
         st = self._lib.sj_probe_gather(
-            self.handle, ctypes.byref(key), 1, _cols(pin), len(pin), None if attached else _cols(bin_), n_bin,
+            self.handle, kcols, nkeys, _cols(pin), len(pin), None if attached else _cols(bin_), n_bin,
             out.probe_rid.data_ptr() if out.probe_rid is not None else None,
             out.build_rid.data_ptr() if out.build_rid is not None else None,
             _cols(pout, L.SjMutColumn), _cols(bout, L.SjMutColumn), capacity, None, _stream_handle(stream),
@@ -230,8 +242,9 @@ class HashTable:
 
         Outer rows carry ``SJ_NO_ROW`` as the missing side's row id and NULL payloads; LEFT/FULL
         outputs get validity buffers for every padded payload column. Synchronizes."""
-        dev = probe_keys.device
-        n = probe_keys.numel()
+        kcols, nkeys, first = _keys(probe_keys, probe_validity)
+        dev = first.device
+        n = first.numel()
         if kind == L.SJ_JOIN_INNER:
             return self.probe_gather(probe_keys, probe_validity, probe_payload, build_payload, attached=attached,
                                      capacity=capacity, stream=stream)
@@ -273,9 +286,8 @@ class HashTable:
         pout = [_mut(t, v) for t, v in zip(out.probe_payload, out.probe_payload_validity)]
         bout = [_mut(t, v) for t, v in zip(out.build_payload, out.build_payload_validity)]
         dc = torch.empty(1, dtype=torch.int64, device=dev)
-        key = make_column(probe_keys, probe_validity)
         st = self._lib.sj_probe_join(
-            self.handle, kind, ctypes.byref(key), 1, _cols(pin), len(pin), None if attached else _cols(bin_), n_bin,
+            self.handle, kind, kcols, nkeys, _cols(pin), len(pin), None if attached else _cols(bin_), n_bin,
             out.probe_rid.data_ptr() if out.probe_rid is not None else None,
             out.build_rid.data_ptr() if out.build_rid is not None else None,
             _cols(pout, L.SjMutColumn), _cols(bout, L.SjMutColumn), capacity,

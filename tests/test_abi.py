@@ -92,9 +92,9 @@ def test_argument_validation_needs_no_gpu(built):
     col = _lib.SjColumn()
     col.type = _lib.SJ_INT32
     out = ctypes.c_void_p()
-    st = lib.sj_build(ctypes.byref(col), 2, None, None, None, ctypes.byref(out))
+    st = lib.sj_build(ctypes.byref(col), 5, None, None, None, ctypes.byref(out))
     assert st == _lib.SJ_ERR_INVALID
-    assert b"one key column" in lib.sj_last_error()
+    assert b"1 to 4 key columns" in lib.sj_last_error()
     col.type = _lib.SJ_FLOAT32
     st = lib.sj_build(ctypes.byref(col), 1, None, None, None, ctypes.byref(out))
     assert st == _lib.SJ_ERR_INVALID

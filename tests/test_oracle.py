@@ -182,3 +182,16 @@ def test_kind_join_partitions_the_probe_rows():
     assert len(pr) == O.hash_join_count(bk, pk, bv, pv) + len(a)
     pr, br = O.kind_join("full", bk, pk, bv, pv)
     assert np.all(np.isin(np.arange(1000), br))  # every build row appears in a FULL join
+
+
+def test_composite_keys_reduce_tuples_to_ids():
+    b = [np.array([1, 1, 2, 2], np.int64), np.array([10, 20, 10, 20], np.int32)]
+    p = [np.array([1, 2, 2, 3], np.int64), np.array([20, 10, 30, 10], np.int32)]
+    bv = [None, O.pack_validity(np.array([True, True, False, True]))]
+    bi, pi, bvw, pvw = O.composite_keys(b, p, bv, None)
+    r = O.hash_join(bi, pi, bvw, pvw)
+    pairs = sorted(zip(r.probe_rid.tolist(), r.build_rid.tolist()))
+    assert pairs == [(0, 1)]  # (1,20) matches build row 1; build row 2 has a NULL component
+    bi, pi, _, _ = O.composite_keys(b, p, bv, None, nulls_equal=True)
+    r = O.hash_join(bi, pi)
+    assert sorted(zip(r.probe_rid.tolist(), r.build_rid.tolist())) == [(0, 1)]

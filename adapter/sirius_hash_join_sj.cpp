@@ -99,6 +99,14 @@ sj_column to_sj(cudf::column_view const& c) {
   return s;
 }
 
+// The equi-key columns of a condition (1..4 INT32/INT64 columns; several form a composite key).
+std::vector<sj_column> key_columns(cudf::table_view const& keys) {
+  if (keys.num_columns() < 1 || keys.num_columns() > 4) throw std::runtime_error("sj adapter: 1 to 4 equi-key columns");
+  std::vector<sj_column> out;
+  for (cudf::size_type c = 0; c < keys.num_columns(); ++c) out.push_back(to_sj(keys.column(c)));
+  return out;
+}
+
 void check(sj_status st, char const* where) {
   if (st == SJ_OK) return;
   const std::string msg = std::string(where) + ": " + sj_status_string(st) + ": " + sj_last_error();
@@ -111,8 +119,7 @@ sj_hash_table::sj_hash_table(cudf::table_view const& build_keys, cudf::table_vie
                              rmm::device_async_resource_ref mr)
   : mr_(mr), stream_(stream)
 {
-  if (build_keys.num_columns() != 1) throw std::runtime_error("sj adapter: one equi-key column");
-  const sj_column key = to_sj(build_keys.column(0));
+  const std::vector<sj_column> keys = key_columns(build_keys);
   std::vector<sj_column> pay;
   for (cudf::size_type c = 0; c < build_payload.num_columns(); ++c) {
     pay.push_back(to_sj(build_payload.column(c)));
@@ -126,7 +133,8 @@ sj_hash_table::sj_hash_table(cudf::table_view const& build_keys, cudf::table_vie
   rmm_alloc_ctx ctx{mr};
   const sj_alloc a{&ctx, rmm_alloc, rmm_free};
   // sj_build_ex synchronizes the stream, as the operator does after building (:1622)
-  check(sj_build_ex(&key, 1, pay.data(), (int32_t)pay.size(), &p, &a, raw(stream), &table_), "sj_build_ex");
+  check(sj_build_ex(keys.data(), (int32_t)keys.size(), pay.data(), (int32_t)pay.size(), &p, &a, raw(stream), &table_),
+        "sj_build_ex");
 }
 
 sj_hash_table::~sj_hash_table() { sj_table_destroy(table_, raw(stream_)); }
@@ -163,8 +171,8 @@ std::unique_ptr<cudf::table> sj_hash_table::run(sj_join_kind kind, cudf::table_v
                                                 cudf::table_view const* build_cols, rmm::cuda_stream_view stream,
                                                 rmm::device_async_resource_ref mr) const
 {
-  if (probe_keys.num_columns() != 1) throw std::runtime_error("sj adapter: one equi-key column");
-  const sj_column key = to_sj(probe_keys.column(0));
+  const std::vector<sj_column> keys = key_columns(probe_keys);
+  const sj_column& key = keys[0];
   rmm_alloc_ctx ctx{mr};
   const sj_alloc a{&ctx, rmm_alloc, rmm_free};
   const bool outer_build = kind == SJ_JOIN_LEFT || kind == SJ_JOIN_FULL;  // build side NULL-padded
@@ -178,7 +186,8 @@ std::unique_ptr<cudf::table> sj_hash_table::run(sj_join_kind kind, cudf::table_v
   rmm::device_buffer d_count(sizeof(int64_t), stream, mr);
   int64_t inner = key.num_rows;
   if (info.layout != SJ_LAYOUT_DISTINCT && kind != SJ_JOIN_SEMI && kind != SJ_JOIN_ANTI) {
-    check(sj_probe_count(table_, &key, 1, &a, raw(stream), static_cast<int64_t*>(d_count.data())), "sj_probe_count");
+    check(sj_probe_count(table_, keys.data(), (int32_t)keys.size(), &a, raw(stream), static_cast<int64_t*>(d_count.data())),
+          "sj_probe_count");
     cudaMemcpyAsync(&inner, d_count.data(), sizeof(int64_t), cudaMemcpyDeviceToHost, stream.value());
     cudaStreamSynchronize(stream.value());
   }
@@ -216,7 +225,7 @@ std::unique_ptr<cudf::table> sj_hash_table::run(sj_join_kind kind, cudf::table_v
     for (size_t c = 0; c < build_types_.size(); ++c) add_out(build_types_[c], outer_build || build_nullable_[c], bout);
   }
 
-  check(sj_probe_join(table_, kind, &key, 1, pin.data(), (int32_t)pin.size(),
+  check(sj_probe_join(table_, kind, keys.data(), (int32_t)keys.size(), pin.data(), (int32_t)pin.size(),
                       build_cols ? bin.data() : nullptr /* NULL: the attached build columns */, (int32_t)bout.size(),
                       nullptr, nullptr, pout.data(), bout.data(), capacity, nullptr, nullptr, &a, raw(stream),
                       static_cast<int64_t*>(d_count.data())),
@@ -243,15 +252,16 @@ std::unique_ptr<cudf::table> sj_hash_table::mark_join(cudf::table_view const& pr
                                                       rmm::cuda_stream_view stream,
                                                       rmm::device_async_resource_ref mr) const
 {
-  if (probe_keys.num_columns() != 1) throw std::runtime_error("sj adapter: one equi-key column");
-  const sj_column key = to_sj(probe_keys.column(0));
+  const std::vector<sj_column> keys = key_columns(probe_keys);
+  const sj_column& key = keys[0];
   rmm_alloc_ctx ctx{mr};
   const sj_alloc a{&ctx, rmm_alloc, rmm_free};
   const auto n = static_cast<cudf::size_type>(key.num_rows);
   rmm::device_buffer d_count(sizeof(int64_t), stream, mr);
   rmm::device_buffer mark((size_t)n, stream, mr);
   rmm::device_buffer mask((size_t)((n + 31) / 32) * sizeof(uint32_t), stream, mr);
-  check(sj_probe_join(table_, SJ_JOIN_MARK, &key, 1, nullptr, 0, nullptr, 0, nullptr, nullptr, nullptr, nullptr, 0,
+  check(sj_probe_join(table_, SJ_JOIN_MARK, keys.data(), (int32_t)keys.size(), nullptr, 0, nullptr, 0, nullptr, nullptr,
+                      nullptr, nullptr, 0,
                       static_cast<uint8_t*>(mark.data()), static_cast<uint32_t*>(mask.data()), &a, raw(stream),
                       static_cast<int64_t*>(d_count.data())),
         "sj_probe_join");

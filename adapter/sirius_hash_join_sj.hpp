@@ -1,6 +1,6 @@
 // Sirius-side glue for the sm_100a equi-join: what `sirius_physical_hash_join::execute`
 // (src/op/sirius_physical_hash_join.cpp:1527-1955) calls instead of cuDF for its equi-joins
-// (INNER, LEFT, SEMI, ANTI, MARK, FULL on one key column).
+// (INNER, LEFT, SEMI, ANTI, MARK, FULL on 1..4 INT32/INT64 key columns).
 //
 // It maps cudf::column_view to sj_column, wraps the task's RMM resource as an sj_alloc (so the
 // join's device memory is charged to the task's cuCascade reservation,
@@ -27,6 +27,9 @@ sj_type to_sj_type(cudf::data_type t);
 
 /// Read-only view of a column: data at row 0, the null mask with the view's bit offset.
 sj_column to_sj(cudf::column_view const& c);
+
+/// The equi-key columns of a join condition as sj_columns (1..4; several form a composite key).
+std::vector<sj_column> key_columns(cudf::table_view const& keys);
 
 /// Throws rmm::out_of_memory for SJ_ERR_OOM, std::runtime_error otherwise (no-op for SJ_OK).
 void check(sj_status st, char const* where);

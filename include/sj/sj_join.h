@@ -295,6 +295,20 @@ SJ_EXPORT sj_status sj_probe_join(const sj_table* table, sj_join_kind kind, cons
                                   uint32_t* out_mark_validity, const sj_alloc* alloc, sj_stream_t stream,
                                   int64_t* d_count);
 
+/* Hash partitioning of a table (the partition operator's hash_partition,
+ * src/op/partition/gpu_partition_impl.cpp:29-110, which splits both sides of a partitioned join).
+ * The `num_columns` columns (up to 8; include the key columns to have them reordered too) are written
+ * to out_columns in partition order; partition p occupies rows [d_offsets[p], d_offsets[p+1]) and
+ * d_offsets (device, num_partitions + 1 int64) ends with the row count. The partition of a row is
+ * the top log2(num_partitions) bits of mix64 of its key — the key itself for one key column without
+ * NULLs (the same function that splits a radix-partitioned table), else a fold over the 1..4 key
+ * columns; rows with a NULL key column go to partition 0. Equal keys land in the same partition in
+ * every table. num_partitions: a power of two, 1..1024. Order within a partition is unspecified.
+ * Stream-ordered; scratch from `alloc`. */
+SJ_EXPORT sj_status sj_hash_partition(const sj_column* keys, int32_t num_keys, const sj_column* columns,
+                                      int32_t num_columns, int32_t num_partitions, const sj_mut_column* out_columns,
+                                      int64_t* d_offsets, const sj_alloc* alloc, sj_stream_t stream);
+
 /* One-shot INNER join (STANDARD mode: cudf::inner_join(left_keys, right_keys, compare_nulls(),
  * stream), src/op/sirius_physical_hash_join.cpp:1872, followed by gather_join_output): builds a
  * throwaway table on build_keys, probes it with probe_keys and gathers. Same output contract as

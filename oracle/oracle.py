@@ -266,6 +266,30 @@ def composite_keys(build_cols, probe_cols, build_valid=None, probe_valid=None, n
     return ids[:nb], ids[nb:], pack_validity(all_valid[:nb]), pack_validity(all_valid[nb:])
 
 
+def partition_ids(key_cols, key_valid=None, num_partitions=1):
+    """Partition of every row under the partition operator's rule: the top log2(P) bits of mix64 of
+    the key — the key itself for one column without NULLs, else the fold k0, mix64(h) ^ k_c, with
+    0 for a row with any NULL key column."""
+    n = len(key_cols[0])
+    key_valid = key_valid or [None] * len(key_cols)
+    bits = int(num_partitions).bit_length() - 1
+    vals = [np.asarray(c).astype(np.int64).view(np.uint64) for c in key_cols]
+    if len(key_cols) == 1 and key_valid[0] is None:
+        h = vals[0]
+    else:
+        h = vals[0].copy()
+        for v in vals[1:]:
+            h = _mix(h) ^ v
+        null = np.zeros(n, bool)
+        for kv in key_valid:
+            if kv is not None:
+                null |= ~unpack_validity(kv, n)
+        h[null] = np.uint64(0)
+    if bits == 0:
+        return np.zeros(n, np.int64)
+    return (_mix(h) >> np.uint64(64 - bits)).astype(np.int64)
+
+
 # ------------------------------------------------------------------------------------------------
 # Canonical form and order-independent checksum
 # ------------------------------------------------------------------------------------------------

@@ -108,6 +108,8 @@ SIGNATURES = {
     "sj_probe_join": (c_int32, [c_void_p, c_int32, _P(SjColumn), c_int32, _P(SjColumn), c_int32, _P(SjColumn),
                                 c_int32, c_void_p, c_void_p, _P(SjMutColumn), _P(SjMutColumn), c_int64, c_void_p,
                                 c_void_p, _P(SjAlloc), c_void_p, c_void_p]),
+    "sj_hash_partition": (c_int32, [_P(SjColumn), c_int32, _P(SjColumn), c_int32, c_int32, _P(SjMutColumn),
+                                    c_void_p, _P(SjAlloc), c_void_p]),
     "sj_status_string": (c_char_p, [c_int32]),
     "sj_last_error": (c_char_p, []),
     "sj_version": (c_int32, []),

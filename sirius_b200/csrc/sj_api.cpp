@@ -331,6 +331,19 @@ SJ_EXPORT sj_status sj_probe_join(const sj_table* table, sj_join_kind kind, cons
   }
 }
 
+SJ_EXPORT sj_status sj_hash_partition(const sj_column* keys, int32_t num_keys, const sj_column* columns,
+                                      int32_t num_columns, int32_t num_partitions, const sj_mut_column* out_columns,
+                                      int64_t* d_offsets, const sj_alloc* alloc, sj_stream_t stream) {
+  clear_error();
+  if (!keys || (num_columns > 0 && !columns)) return set_error(SJ_ERR_INVALID, "keys and columns are required");
+  try {
+    return hash_partition(keys, num_keys, columns, num_columns, num_partitions, out_columns, d_offsets,
+                          Allocator(alloc), reinterpret_cast<cudaStream_t>(stream));
+  } catch (const std::exception& e) {
+    return set_error(SJ_ERR_DEVICE, e.what());
+  }
+}
+
 SJ_EXPORT sj_status sj_inner_join(const sj_column* build_keys, const sj_column* probe_keys, int32_t num_keys,
                                   const sj_column* probe_payload, int32_t num_probe_payload,
                                   const sj_column* build_payload, int32_t num_build_payload, int32_t* out_probe_rid,

@@ -187,6 +187,10 @@ sj_status pack_build_keys(const sj_column* keys, int n_keys, bool nulls_equal, c
 sj_status pack_probe_keys(const KeyPack& kp, const sj_column* keys, int n_keys, const Allocator& alloc,
                           cudaStream_t s, Scratch& buf, sj_column* packed);
 
+// Hash partitioning of a table (sj_partition_op.cu).
+sj_status hash_partition(const sj_column* keys, int n_keys, const sj_column* cols, int n_cols, int n_parts,
+                         const sj_mut_column* out, int64_t* d_offsets, const Allocator& alloc, cudaStream_t s);
+
 // LEFT / SEMI / ANTI / MARK / FULL (sj_probe_kinds.cu); INNER delegates to probe_gather.
 sj_status probe_join(const sj_table* t, int32_t kind, const sj_column& probe, const GatherSpec& g, uint8_t* out_mark,
                      uint32_t* out_mark_valid, const Allocator& alloc, cudaStream_t stream, int64_t* d_count);

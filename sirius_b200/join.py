@@ -325,3 +325,23 @@ def inner_join(build_keys, probe_keys, build_validity=None, probe_validity=None,
     with HashTable(build_keys, build_validity, stream=stream, **table_kwargs) as t:
         return t.probe_gather(probe_keys, probe_validity, probe_payload, build_payload, capacity=capacity,
                               stream=stream).trimmed()
+
+
+def hash_partition(keys, columns, num_partitions: int, stream: Optional[torch.cuda.Stream] = None):
+    """Reorder `columns` (tensors or (tensor, validity) pairs) by the hash partition of `keys` (a
+    tensor, or a list of 1..4 key columns / pairs). Returns (partitioned columns, partitioned validity
+    words or None per column, offsets: int64 tensor of num_partitions + 1)."""
+    lib = L.load()
+    kcols, nkeys, first = _keys(keys)
+    dev = first.device
+    n = first.numel()
+    pairs = [_as_pair(c) for c in columns]
+    ins = [make_column(t, v) for t, v in pairs]
+    outs = [torch.empty(n, dtype=t.dtype, device=dev) for t, _ in pairs]
+    vouts = [torch.empty((n + 31) // 32, dtype=torch.int32, device=dev) if v is not None else None for _, v in pairs]
+    offsets = torch.empty(num_partitions + 1, dtype=torch.int64, device=dev)
+    st = lib.sj_hash_partition(kcols, nkeys, _cols(ins), len(ins), num_partitions,
+                               _cols([_mut(t, v) for t, v in zip(outs, vouts)], L.SjMutColumn), offsets.data_ptr(),
+                               None, _stream_handle(stream))
+    L.check(st, "sj_hash_partition")
+    return outs, vouts, offsets

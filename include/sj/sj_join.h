@@ -309,6 +309,22 @@ SJ_EXPORT sj_status sj_hash_partition(const sj_column* keys, int32_t num_keys, c
                                       int32_t num_columns, int32_t num_partitions, const sj_mut_column* out_columns,
                                       int64_t* d_offsets, const sj_alloc* alloc, sj_stream_t stream);
 
+/* Dynamic filter from the build keys (src/cuda/sirius_dynamic_bloom_filter.cu, published by the
+ * hash join at src/op/sirius_physical_hash_join.cpp:1960-2069): a blocked Bloom filter of 32-byte
+ * blocks, `bits_per_key` bits per key (0 = 16), 8 bits set per key in one block, so a probe row is
+ * tested with one sector read. NULL keys are not inserted. sj_bloom_contains writes one byte per
+ * probe row: 1 = may be in the build keys (no false negatives), 0 = not; rows with a NULL probe key
+ * test 0 and, when out_validity is given, get a NULL bit there (the probe's NULLs). For an exact
+ * in-list filter use a built table: sj_probe_join(SJ_JOIN_MARK) gives the same mask without false
+ * positives. Stream-ordered. */
+typedef struct sj_bloom sj_bloom;
+SJ_EXPORT sj_status sj_bloom_build(const sj_column* keys, int32_t bits_per_key, const sj_alloc* alloc,
+                                   sj_stream_t stream, sj_bloom** out);
+SJ_EXPORT sj_status sj_bloom_contains(const sj_bloom* bloom, const sj_column* probe_keys, uint8_t* out_mask,
+                                      uint32_t* out_validity, sj_stream_t stream);
+SJ_EXPORT int64_t sj_bloom_bytes(const sj_bloom* bloom);
+SJ_EXPORT sj_status sj_bloom_destroy(sj_bloom* bloom, sj_stream_t stream);
+
 /* One-shot INNER join (STANDARD mode: cudf::inner_join(left_keys, right_keys, compare_nulls(),
  * stream), src/op/sirius_physical_hash_join.cpp:1872, followed by gather_join_output): builds a
  * throwaway table on build_keys, probes it with probe_keys and gathers. Same output contract as

@@ -290,6 +290,39 @@ def partition_ids(key_cols, key_valid=None, num_partitions=1):
     return (_mix(h) >> np.uint64(64 - bits)).astype(np.int64)
 
 
+def bloom_mask(bkeys, pkeys, bvalid=None, pvalid=None, bits_per_key=16):
+    """The blocked Bloom filter's answer per probe row (uint8), restated in numpy: 2^b blocks of 8
+    32-bit words (the smallest b with 256 * 2^b >= keys * bits_per_key), block = top b bits of
+    mix64(key), bit of word w = bits [5w, 5w+5) of mix64(mix64(key) + 0x9E3779B97F4A7C15); NULL keys
+    are not inserted and test 0."""
+    nb, npr = len(bkeys), len(pkeys)
+    want = max(nb, 1) * bits_per_key
+    b = 0
+    while b < 40 and (256 << b) < want:
+        b += 1
+    words = np.zeros((1 << b) * 8, np.uint32)
+
+    def locate(keys):
+        h = _mix(np.asarray(keys).astype(np.int64).view(np.uint64))
+        block = (h >> np.uint64(64 - b)) if b else np.zeros(len(h), np.uint64)
+        with np.errstate(over="ignore"):
+            bits = _mix(h + np.uint64(0x9E3779B97F4A7C15))
+        return block.astype(np.int64), bits
+
+    ok = unpack_validity(bvalid, nb) if bvalid is not None else np.ones(nb, bool)
+    blk, bits = locate(bkeys)
+    for w in range(8):
+        bit = ((bits >> np.uint64(5 * w)) & np.uint64(31)).astype(np.uint32)
+        np.bitwise_or.at(words, blk[ok] * 8 + w, (np.uint32(1) << bit[ok]))
+    pok = unpack_validity(pvalid, npr) if pvalid is not None else np.ones(npr, bool)
+    blk, bits = locate(pkeys)
+    hit = pok.copy()
+    for w in range(8):
+        bit = ((bits >> np.uint64(5 * w)) & np.uint64(31)).astype(np.uint32)
+        hit &= ((words[blk * 8 + w] >> bit) & 1).astype(bool)
+    return hit.astype(np.uint8)
+
+
 # ------------------------------------------------------------------------------------------------
 # Canonical form and order-independent checksum
 # ------------------------------------------------------------------------------------------------

@@ -110,6 +110,10 @@ SIGNATURES = {
                                 c_void_p, _P(SjAlloc), c_void_p, c_void_p]),
     "sj_hash_partition": (c_int32, [_P(SjColumn), c_int32, _P(SjColumn), c_int32, c_int32, _P(SjMutColumn),
                                     c_void_p, _P(SjAlloc), c_void_p]),
+    "sj_bloom_build": (c_int32, [_P(SjColumn), c_int32, _P(SjAlloc), c_void_p, _P(c_void_p)]),
+    "sj_bloom_contains": (c_int32, [c_void_p, _P(SjColumn), c_void_p, c_void_p, c_void_p]),
+    "sj_bloom_bytes": (c_int64, [c_void_p]),
+    "sj_bloom_destroy": (c_int32, [c_void_p, c_void_p]),
     "sj_status_string": (c_char_p, [c_int32]),
     "sj_last_error": (c_char_p, []),
     "sj_version": (c_int32, []),

@@ -345,3 +345,48 @@ def hash_partition(keys, columns, num_partitions: int, stream: Optional[torch.cu
                                None, _stream_handle(stream))
     L.check(st, "sj_hash_partition")
     return outs, vouts, offsets
+
+
+class BloomFilter:
+    """Dynamic filter from build keys (``sj_bloom_build``); ``contains`` gives the per-row mask."""
+
+    def __init__(self, keys: torch.Tensor, validity: Optional[torch.Tensor] = None, bits_per_key: int = 16,
+                 stream: Optional[torch.cuda.Stream] = None):
+        self._lib = L.load()
+        self._h = ctypes.c_void_p()
+        col = make_column(keys, validity)
+        L.check(self._lib.sj_bloom_build(ctypes.byref(col), bits_per_key, None, _stream_handle(stream),
+                                         ctypes.byref(self._h)), "sj_bloom_build")
+
+    @property
+    def nbytes(self) -> int:
+        return int(self._lib.sj_bloom_bytes(self._h))
+
+    def contains(self, probe_keys: torch.Tensor, probe_validity: Optional[torch.Tensor] = None,
+                 stream: Optional[torch.cuda.Stream] = None):
+        """(uint8 mask per row, validity words or None)."""
+        n = probe_keys.numel()
+        mask = torch.empty(n, dtype=torch.uint8, device=probe_keys.device)
+        valid = torch.empty((n + 31) // 32, dtype=torch.int32, device=probe_keys.device) if probe_validity is not None else None
+        col = make_column(probe_keys, probe_validity)
+        L.check(self._lib.sj_bloom_contains(self._h, ctypes.byref(col), mask.data_ptr() if n else None,
+                                            valid.data_ptr() if valid is not None else None,
+                                            _stream_handle(stream)), "sj_bloom_contains")
+        return mask, valid
+
+    def close(self):
+        if self._h:
+            self._lib.sj_bloom_destroy(self._h, None)
+            self._h = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

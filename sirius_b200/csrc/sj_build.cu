@@ -417,8 +417,8 @@ sj_status build_table(const sj_column& keys, const sj_column* payload, int32_t n
     return set_error(SJ_ERR_INVALID, "partition_bits must be 0 (automatic), -1 (never) or in [1, 10]");
   if (p.probe_kernel < SJ_PROBE_KERNEL_AUTO || p.probe_kernel > SJ_PROBE_KERNEL_DIRECT_TMA)
     return set_error(SJ_ERR_INVALID, "unknown probe_kernel");
-  if (p.rows_per_lane != 0 && p.rows_per_lane != 2 && p.rows_per_lane != 4)
-    return set_error(SJ_ERR_INVALID, "rows_per_lane must be 0 (default), 2 or 4");
+  if (p.rows_per_lane != 0 && (p.rows_per_lane < 2 || p.rows_per_lane > 4))
+    return set_error(SJ_ERR_INVALID, "rows_per_lane must be 0 (default), 2, 3 or 4");
   if (n_payload < 0 || n_payload > kMaxPayload || (n_payload > 0 && payload == nullptr))
     return set_error(SJ_ERR_INVALID, "at most 8 attached payload columns");
   for (int c = 0; c < n_payload; ++c) {

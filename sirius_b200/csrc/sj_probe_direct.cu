@@ -77,7 +77,7 @@ __device__ __forceinline__ uint64_t rec_word_field(const uint32_t (&w)[8], int o
 }
 
 template <typename K, bool WIDE, int R, int AGG, int SP = -1, int SB = -1>
-__global__ void __launch_bounds__(kDirectThreads, (R <= 2 ? 1024 : 512) / kDirectThreads)
+__global__ void __launch_bounds__(kDirectThreads, (R <= 2 ? 1024 : R == 3 ? 768 : 512) / kDirectThreads)
     probe_direct_kernel(TableDev t, const K* __restrict__ keys, const uint32_t* __restrict__ kv, int64_t kvoff,
                         int64_t n_host, const int64_t* d_n, DirectArgs a) {
   using Ops = SlotOps<WIDE>;
@@ -569,15 +569,18 @@ static void launch_direct_kernel(const sj_table* t, const sj_column& p, const in
   fixed_shape(a, sp, sb);
   // the shapes of the large foreign-key join (1 probe, 2 build payloads) and of a served lookup
   // (1 build payload) get compile-time specialisations when 2 rows per lane are used
-  if (R == 2 && sp == 1 && sb == 2) return launch_direct_shape<K, WIDE, R, CTA, 1, 2>(t, p, d_n, a, s);
-  if (R == 2 && sp == 0 && sb == 1) return launch_direct_shape<K, WIDE, R, CTA, 0, 1>(t, p, d_n, a, s);
+  if (R <= 3 && sp == 1 && sb == 2) return launch_direct_shape<K, WIDE, R, CTA, 1, 2>(t, p, d_n, a, s);
+  if (R <= 3 && sp == 0 && sb == 1) return launch_direct_shape<K, WIDE, R, CTA, 0, 1>(t, p, d_n, a, s);
   launch_direct_shape<K, WIDE, R, CTA, -1, -1>(t, p, d_n, a, s);
 }
 
 template <typename K, bool WIDE>
 static void launch_direct(const sj_table* t, const sj_column& p, const int64_t* d_n, const DirectArgs& a, int rpl,
                           int mode, cudaStream_t s) {
-  if (rpl >= 4) {
+  if (rpl == 3) {
+    if (mode == 1) launch_direct_kernel<K, WIDE, 3, 1>(t, p, d_n, a, s);
+    else launch_direct_kernel<K, WIDE, 3, 0>(t, p, d_n, a, s);
+  } else if (rpl >= 4) {
     if (mode == 1) launch_direct_kernel<K, WIDE, 4, 1>(t, p, d_n, a, s);
     else launch_direct_kernel<K, WIDE, 4, 0>(t, p, d_n, a, s);
   } else {

@@ -48,3 +48,52 @@ def max_over_ranks(x: float, device=None) -> float:
 def weak_scaling_value(rows_per_rank_per_step: int, steps: int, world: int, max_ms: float) -> float:
     """Job throughput in M rows/s: every rank's rows over the slowest rank's time."""
     return rows_per_rank_per_step * steps * world / (max_ms / 1e3) / 1e6
+
+
+# ------------------------------------------------------------------------------------------------
+# Hash-partitioned join across ranks: one all-to-all exchange, then independent local joins
+# ------------------------------------------------------------------------------------------------
+def gpu_partitioner(keys, columns, world: int):
+    """Partition step on the GPU: sj_hash_partition over `world` partitions (a power of two).
+    Returns (partitioned columns, per-partition row counts as a CPU int64 tensor)."""
+    from . import join as J
+    outs, _, offsets = J.hash_partition(keys, columns, world)
+    return outs, (offsets[1:] - offsets[:-1]).cpu()
+
+
+def exchange(keys, columns, partitioner=gpu_partitioner, group=None):
+    """All-to-all by hash partition (the exchange step of a partitioned join: both sides hash-
+    partitioned on h(key) mod world, one grouped all-to-all, then local joins — over NCCL on GPUs,
+    any torch.distributed backend here). `keys` (one tensor, no NULLs) and `columns` (tensors of the
+    same length) are this rank's rows; returns (keys, columns) of the rows every rank sent here,
+    i.e. this rank's partition of the union. The partition counts go first (one small all-to-all),
+    then each column in one all_to_all_single with those splits."""
+    import torch
+    import torch.distributed as dist
+    world = dist.get_world_size(group)
+    parts, send_counts = partitioner(keys, [keys] + list(columns), world)
+    send_counts = send_counts.to(torch.int64)
+    dev = keys.device
+    sc = send_counts.to(dev)
+    rc = torch.empty_like(sc)
+    dist.all_to_all_single(rc, sc, group=group)
+    recv_counts = rc.cpu()
+    send_splits = [int(x) for x in send_counts]
+    recv_splits = [int(x) for x in recv_counts]
+    received = []
+    for col in parts:
+        out = torch.empty(sum(recv_splits), dtype=col.dtype, device=dev)
+        dist.all_to_all_single(out, col.contiguous(), recv_splits, send_splits, group=group)
+        received.append(out)
+    return received[0], received[1:]
+
+
+def partitioned_inner_join(build_keys, build_cols, probe_keys, probe_cols, local_join,
+                           partitioner=gpu_partitioner, group=None):
+    """INNER join of row-sharded tables across ranks (keys without NULLs: a NULL key never matches,
+    so such rows are dropped before the exchange): exchange both sides by hash partition, then
+    `local_join(build_keys, build_cols, probe_keys, probe_cols)` on this rank's partition. Every
+    matching pair lands on exactly one rank (equal keys share a partition)."""
+    bk, bc = exchange(build_keys, build_cols, partitioner, group)
+    pk, pc = exchange(probe_keys, probe_cols, partitioner, group)
+    return local_join(bk, bc, pk, pc)

@@ -57,3 +57,64 @@ def test_two_ranks_gloo():
     assert v0 == v1 == pytest.approx(50_000 * 4 * 2 / 0.015 / 1e6)
     assert s0 != s1                               # each rank probes its own shard
     assert w0 == w1 == 2
+
+
+def _exchange_worker(rank, world, port, q):
+    import sys
+    from pathlib import Path
+    sys.path.insert(0, str(Path(__file__).resolve().parent.parent))
+    import torch
+    import torch.distributed as dist
+    from oracle import oracle as O
+    from sirius_b200 import multigpu as M
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank), WORLD_SIZE=str(world))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+
+    def cpu_partitioner(keys, columns, w):
+        # the partition rule of sj_hash_partition (the oracle's restatement), applied on the host
+        part = O.partition_ids([keys.numpy()], [None], w)
+        order = np.argsort(part, kind="stable")
+        counts = np.bincount(part, minlength=w)
+        return [c[torch.from_numpy(order)] for c in columns], torch.from_numpy(counts.astype(np.int64))
+
+    def local_join(bk, bc, pk, pc):
+        r = O.hash_join(bk.numpy(), pk.numpy(), probe_payload=[pc[0].numpy()], build_payload=[bc[0].numpy()],
+                        threads=1)
+        return [r.probe_payload[0], r.build_payload[0]]
+
+    try:
+        rng = np.random.default_rng([9, rank])
+        bk = rng.integers(0, 3000, 4000).astype(np.int64)       # duplicates across ranks
+        pk = rng.integers(-50, 3500, 9000).astype(np.int64)
+        bid = (rank * 10_000_000 + np.arange(len(bk))).astype(np.int64)  # global row ids as payloads
+        pid = (rank * 10_000_000 + np.arange(len(pk))).astype(np.int64)
+        out = M.partitioned_inner_join(torch.from_numpy(bk), [torch.from_numpy(bid)], torch.from_numpy(pk),
+                                       [torch.from_numpy(pid)], local_join, partitioner=cpu_partitioner)
+        q.put((rank, out[0].tolist(), out[1].tolist(), bk.tolist(), pk.tolist()))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_partitioned_exchange_join_gloo():
+    """The union over ranks of the local joins after the hash exchange equals the global INNER join
+    of the sharded tables (as (probe global id, build global id) pairs), with no pair twice."""
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    world = 2
+    procs = [ctx.Process(target=_exchange_worker, args=(r, world, port, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    res = sorted(q.get(timeout=180) for _ in procs)
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    from oracle import oracle as O
+    got = sorted(pair for r in res for pair in zip(r[1], r[2]))
+    bk = np.concatenate([np.array(r[3], np.int64) for r in res])
+    pk = np.concatenate([np.array(r[4], np.int64) for r in res])
+    bid = np.concatenate([r[0] * 10_000_000 + np.arange(len(r[3])) for r in res]).astype(np.int64)
+    pid = np.concatenate([r[0] * 10_000_000 + np.arange(len(r[4])) for r in res]).astype(np.int64)
+    ref = O.hash_join(bk, pk, threads=2)
+    exp = sorted(zip(pid[ref.probe_rid].tolist(), bid[ref.build_rid].tolist()))
+    assert got == exp and len(set(got)) == len(got)

@@ -256,7 +256,9 @@ static FastSmem fast_smem(int pbits, int kw, int n_pay) {
   return m;
 }
 
-static bool fast_scatter_ok(const PartSrc& s, const PartDst& d) {
+bool partition_plain_shape(const PartSrc& s, const PartDst& d);
+static bool fast_scatter_ok(const PartSrc& s, const PartDst& d) { return partition_plain_shape(s, d); }
+bool partition_plain_shape(const PartSrc& s, const PartDst& d) {
   if (d.stride != 0 || s.n_pay > kFastMaxPay) return false;
   for (int c = 0; c < s.n_pay; ++c)
     if (s.pay[c].valid || s.pay[c].valid8 || (s.pay[c].width != 4 && s.pay[c].width != 8) ||
@@ -287,10 +289,13 @@ __device__ __forceinline__ void fast_load_tile(const PartSrc& s, int64_t t0, int
   }
 }
 
-template <typename K, int NP>
+// LOCAL: no global offsets — every tile is written back in place, sorted by partition, and its
+// per-partition runs go to run_off / run_cnt[tile * P + p] (the probe walks them partition-major).
+template <typename K, int NP, bool LOCAL = false>
 __global__ void __launch_bounds__(kPartThreads, 3) part_scatter_fast_kernel(PartSrc s, int pbits, int64_t chunk,
                                                                          const int64_t* __restrict__ off, PartDst d,
-                                                                         FastSmem m) {
+                                                                         FastSmem m, int32_t* run_off = nullptr,
+                                                                         int32_t* run_cnt = nullptr) {
   extern __shared__ __align__(16) unsigned char sm[];
   unsigned long long* cur = reinterpret_cast<unsigned long long*>(sm + m.cur);
   unsigned int* tcnt = reinterpret_cast<unsigned int*>(sm + m.tcnt);
@@ -301,7 +306,8 @@ __global__ void __launch_bounds__(kPartThreads, 3) part_scatter_fast_kernel(Part
   __shared__ unsigned int s_wsum[kPartThreads / 32];
   const int P = 1 << pbits;
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
-  for (int p = tid; p < P; p += kPartThreads) cur[p] = (unsigned long long)off[(int64_t)p * gridDim.x + blockIdx.x];
+  if (!LOCAL)
+    for (int p = tid; p < P; p += kPartThreads) cur[p] = (unsigned long long)off[(int64_t)p * gridDim.x + blockIdx.x];
   const int64_t lo = (int64_t)blockIdx.x * chunk;
   const int64_t hi = lo + chunk < s.n ? lo + chunk : s.n;
   K* okeys = static_cast<K*>(d.keys);
@@ -354,6 +360,13 @@ __global__ void __launch_bounds__(kPartThreads, 3) part_scatter_fast_kernel(Part
     }
     unsigned tile_valid = 0;
     for (int w = 0; w < kPartThreads / 32; ++w) tile_valid += s_wsum[w];
+    if (LOCAL) {
+      const int64_t ti = t0 / kTile;
+      for (int p = tid; p < P; p += kPartThreads) {
+        run_off[ti * P + p] = (int32_t)(t0 + toff[p]);
+        run_cnt[ti * P + p] = (int32_t)tcnt[p];
+      }
+    }
     __syncthreads();
     // 3. counting-sort the tile into shared memory (payloads straight to their sorted slot, with
     //    each row's output position, so the write-out reads nothing per partition)
@@ -363,7 +376,7 @@ __global__ void __launch_bounds__(kPartThreads, 3) part_scatter_fast_kernel(Part
       const unsigned slot = toff[pr[j]] + rank[j];
       skey[slot] = kk[j];
       srid[slot] = (int32_t)(t0 + j * kPartThreads + tid);
-      sdst[slot] = (uint32_t)cur[pr[j]] + rank[j];
+      sdst[slot] = LOCAL ? (uint32_t)t0 + slot : (uint32_t)cur[pr[j]] + rank[j];
 #pragma unroll
       for (int c = 0; c < NP; ++c) reinterpret_cast<uint64_t*>(sm + m.pay[c])[slot] = pv[c][j];
     }
@@ -382,8 +395,10 @@ __global__ void __launch_bounds__(kPartThreads, 3) part_scatter_fast_kernel(Part
       }
     }
     __syncthreads();
-    for (int p = tid; p < P; p += kPartThreads) cur[p] += tcnt[p];
-    __syncthreads();
+    if (!LOCAL) {
+      for (int p = tid; p < P; p += kPartThreads) cur[p] += tcnt[p];
+      __syncthreads();
+    }
   }
 }
 
@@ -394,7 +409,7 @@ static sj_status launch_fast_scatter(const PartSrc& src, int pbits, int64_t chun
   auto go = [&](auto kernel) -> sj_status {
     SJ_CUDA_TRY(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)m.total));
     KernelTimer timer("partition_scatter", s);
-    kernel<<<G, kPartThreads, m.total, s>>>(src, pbits, chunk, offs, dst, m);
+    kernel<<<G, kPartThreads, m.total, s>>>(src, pbits, chunk, offs, dst, m, nullptr, nullptr);
     return SJ_OK;
   };
   if (src.n_pay == 0) return go(part_scatter_fast_kernel<K, 0>);
@@ -429,6 +444,39 @@ static int scatter_per_sm(const PartSrc& src, int key_type, int pbits, bool fast
   }
   cudaGetLastError();
   return std::max(1, std::min(4, r));
+}
+
+// Tile-local partition: one pass, no histogram. Returns the number of tiles (run table rows).
+sj_status local_partition(const PartSrc& src, int key_type, int pbits, const PartDst& dst, int32_t* run_off,
+                          int32_t* run_cnt, int device, cudaStream_t s) {
+  if (!fast_scatter_ok(src, dst)) return set_error(SJ_ERR_INVALID, "tile-local partition needs the plain shape");
+  const int P = 1 << pbits;
+  const int64_t tiles = (src.n + kTile - 1) / kTile;
+  const int per_sm = scatter_per_sm(src, key_type, pbits, true);
+  const int64_t G = std::max<int64_t>(1, std::min<int64_t>(tiles, (int64_t)sm_count(device) * per_sm));
+  const int64_t chunk = (tiles + G - 1) / G * kTile;  // whole tiles per CTA
+  const int grid = (int)((src.n + chunk - 1) / chunk);
+  if (src.n == 0) return SJ_OK;
+  auto go = [&](auto kernel) -> sj_status {
+    const FastSmem m = fast_smem(pbits, key_type == SJ_INT32 ? 4 : 8, src.n_pay);
+    SJ_CUDA_TRY(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)m.total));
+    KernelTimer timer("partition_scatter", s);
+    kernel<<<grid, kPartThreads, m.total, s>>>(src, pbits, chunk, nullptr, dst, m, run_off, run_cnt);
+    return SJ_OK;
+  };
+  (void)P;
+  sj_status st;
+  if (key_type == SJ_INT32)
+    st = src.n_pay == 0 ? go(part_scatter_fast_kernel<int32_t, 0, true>)
+       : src.n_pay == 1 ? go(part_scatter_fast_kernel<int32_t, 1, true>)
+                        : go(part_scatter_fast_kernel<int32_t, 2, true>);
+  else
+    st = src.n_pay == 0 ? go(part_scatter_fast_kernel<int64_t, 0, true>)
+       : src.n_pay == 1 ? go(part_scatter_fast_kernel<int64_t, 1, true>)
+                        : go(part_scatter_fast_kernel<int64_t, 2, true>);
+  SJ_TRY(st);
+  SJ_CUDA_TRY(cudaGetLastError());
+  return SJ_OK;
 }
 
 size_t partition_scratch_bytes(int pbits, int device) {

@@ -28,6 +28,14 @@ struct PartDst {
 };
 
 size_t partition_scratch_bytes(int pbits, int device);
+// Tile-local variant (one pass, no histogram): each kTile-row tile (2048) is sorted by partition
+// in place; run_off / run_cnt[tile * 2^pbits + p] give partition p's rows of every tile. Only for
+// plain outputs with at most 2 payloads of 4/8 bytes without NULLs. NULL-key rows are dropped.
+constexpr int kPartTileRows = 2048;
+sj_status local_partition(const PartSrc& src, int key_type, int pbits, const PartDst& dst, int32_t* run_off,
+                          int32_t* run_cnt, int device, cudaStream_t s);
+bool partition_plain_shape(const PartSrc& src, const PartDst& dst);
+
 sj_status radix_partition(const PartSrc& src, int key_type, int pbits, const PartDst& dst, void* scratch,
                           int device, cudaStream_t s, const int64_t** d_total_out, const int64_t** d_offs_out,
                           int* grid_out);

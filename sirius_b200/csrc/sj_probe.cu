@@ -781,7 +781,16 @@ static sj_status probe_partitioned(const sj_table* t, const sj_column& p, Gather
   const int64_t n = p.num_rows;
   const int pbits = probe_partition_bits(t);
   const int kw = t->key_type == SJ_INT32 ? 4 : 8;
-  size_t bytes = align256((size_t)n * kw) + align256((size_t)n * 4) + partition_scratch_bytes(pbits, t->device) + 256;
+  // Tile-local partition (one pass, no histogram) + the run-walking probe, when the direct probe
+  // serves the output shape and the probe payloads are plain 4/8-byte columns without NULLs.
+  bool local = probe_runs_ok(t, g) && g.n_pin <= 2;
+  for (int c = 0; c < g.n_pin; ++c)
+    local = local && !g.pin[c].valid && !g.pin[c].valid8 && (g.pin[c].width == 4 || g.pin[c].width == 8) &&
+            g.pin[c].stride == g.pin[c].width;
+  const int64_t n_tiles = (n + kPartTileRows - 1) / kPartTileRows;
+  const size_t run_bytes = (size_t)n_tiles * ((size_t)1 << pbits) * sizeof(int32_t);
+  size_t bytes = align256((size_t)n * kw) + align256((size_t)n * 4) + 256 +
+                 (local ? 2 * align256(run_bytes) : partition_scratch_bytes(pbits, t->device));
   for (int c = 0; c < g.n_pin; ++c)
     bytes += align256((size_t)n * g.pin[c].width) + (g.pin[c].valid ? align256((size_t)n) : 0);
   Scratch sc;
@@ -806,8 +815,19 @@ static sj_status probe_partitioned(const sj_table* t, const sj_column& p, Gather
     pd.pay[c] = carve((size_t)n * g.pin[c].width);
     pd.valid8[c] = g.pin[c].valid ? reinterpret_cast<uint8_t*>(carve((size_t)n)) : nullptr;
   }
-  void* pscratch = carve(partition_scratch_bytes(pbits, t->device));
   unsigned long long* tile_ctr = reinterpret_cast<unsigned long long*>(carve(8));
+  if (local) {
+    int32_t* run_off = reinterpret_cast<int32_t*>(carve(run_bytes));
+    int32_t* run_cnt = reinterpret_cast<int32_t*>(carve(run_bytes));
+    SJ_TRY(local_partition(ps, t->key_type, pbits, pd, run_off, run_cnt, t->device, s));
+    g.prid_map = pd.rid;
+    for (int c = 0; c < g.n_pin; ++c) g.pin[c] = column_payload(pd.pay[c], nullptr, 0, g.pin[c].width);
+    const RunArgs ra{run_off, run_cnt, (uint32_t)n_tiles, 1u << pbits};
+    probe_runs(t, pd.keys, ra, g, s, tile_ctr);
+    SJ_CUDA_TRY(cudaGetLastError());
+    return SJ_OK;
+  }
+  void* pscratch = carve(partition_scratch_bytes(pbits, t->device));
   const int64_t *d_total, *d_offs;
   int G;
   SJ_TRY(radix_partition(ps, t->key_type, pbits, pd, pscratch, t->device, s, &d_total, &d_offs, &G));

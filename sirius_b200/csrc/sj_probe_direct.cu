@@ -262,6 +262,240 @@ __global__ void __launch_bounds__(kDirectThreads, (R <= 2 ? 1024 : R == 3 ? 768 
 }
 
 // ------------------------------------------------------------------------------------------------
+// The direct probe over tile-local partition runs. A work item is (partition p, 8 consecutive
+// tiles): its rows are the 8 runs of p in those tiles, concatenated; the CTA walks them in chunks of
+// 128 rows (lane l of warp w: chunk rows 64w + 32j + l) mapping each chunk row to its run through a
+// prefix of the 8 run lengths held in shared memory. Items are taken partition-major (all tiles of
+// partition 0 first) from the shared counter, so the CTAs sweep one partition's table rows at a
+// time. Output reservation: one atomicAdd per chunk (two CTA barriers), as in probe_direct_kernel.
+// ------------------------------------------------------------------------------------------------
+constexpr int kRunGroup = 4;
+
+template <typename K, bool WIDE, int SP, int SB>
+__global__ void __launch_bounds__(kDirectThreads, 1024 / kDirectThreads)
+    probe_runs_kernel(TableDev t, const K* __restrict__ keys, RunArgs ra, DirectArgs a) {
+  using Ops = SlotOps<WIDE>;
+  constexpr int R = 2;
+  constexpr bool kFixed = SP >= 0;
+  const int n_pin = kFixed ? SP : a.n_pin;
+  const int n_bin = kFixed ? SB : a.n_bin;
+  const bool use_rec = kFixed ? SB > 0 : a.rec != nullptr;
+  const int rec_stride = kFixed ? (SB == 1 ? 16 : 32) : a.rec_stride;
+  constexpr uint32_t kChunk = (uint32_t)kDirectThreads * R;
+  __shared__ unsigned s_wtot[kDirectWarps];
+  __shared__ unsigned long long s_wbase[kDirectWarps];
+  // two item descriptors: the item being walked and the next one, so a chunk can take the tail
+  // of one item and the head of the next (chunks stay full)
+  __shared__ int32_t s_off[2][kRunGroup];
+  __shared__ int32_t s_pre[2][kRunGroup + 1];
+  __shared__ uint32_t s_after[2];  // the item to load after the one in the slot
+  const int lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
+  const unsigned below = (1u << lane) - 1u;
+  const uint32_t cap = (uint32_t)(a.capacity < (int64_t)INT32_MAX ? a.capacity : (int64_t)INT32_MAX);
+  const uint64_t kmask = ~((1ull << t.rbits) - 1);
+  const uint32_t lane_off = (uint32_t)warp * (32 * R) + lane;
+  const uint32_t n_groups = (ra.n_tiles + kRunGroup - 1) / kRunGroup;
+  const uint32_t n_items = ra.P * n_groups;
+  // warp 0: descriptor of item w into slot `sl` (w >= n_items: an empty item) and the index of the
+  // item after it (taken from the shared counter) into s_after[sl]
+  auto load_item = [&](int sl, uint32_t w) {
+    const bool in = w < n_items;
+    const uint32_t p = in ? w / n_groups : 0, g = in ? w - p * n_groups : 0;
+    const uint32_t ti = g * kRunGroup + lane;
+    const bool ok = in && lane < kRunGroup && ti < ra.n_tiles;
+    const int32_t cnt = ok ? __ldg(ra.run_cnt + (size_t)ti * ra.P + p) : 0;
+    if (lane < kRunGroup) s_off[sl][lane] = ok ? __ldg(ra.run_off + (size_t)ti * ra.P + p) : 0;
+    int32_t incl = cnt;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      const int32_t o = __shfl_up_sync(kFullMask, incl, d);
+      if (lane >= d) incl += o;
+    }
+    if (lane < kRunGroup) s_pre[sl][lane + 1] = incl;
+    if (lane == 0) {
+      s_pre[sl][0] = 0;
+      s_after[sl] = in ? gridDim.x + (uint32_t)atomicAdd(a.tile_ctr, 1ull) : w;
+    }
+  };
+  // chunk row v of the concatenation (slot cur from `base` on, then slot cur ^ 1) -> array position
+  auto row_in = [&](int sl, uint32_t v) -> uint32_t {
+    int q = 0;
+#pragma unroll
+    for (int step = kRunGroup / 2; step > 0; step >>= 1)
+      if ((uint32_t)s_pre[sl][q + step] <= v) q += step;
+    return (uint32_t)s_off[sl][q] + (v - (uint32_t)s_pre[sl][q]);
+  };
+  if (warp == 0) load_item(0, blockIdx.x);
+  __syncthreads();
+  if (warp == 0) load_item(1, s_after[0]);
+  __syncthreads();
+  int cur = 0;
+  uint32_t base = 0;  // rows of item `cur` already taken
+  uint32_t tc = (uint32_t)s_pre[0][kRunGroup], tn = (uint32_t)s_pre[1][kRunGroup];
+  uint32_t w_after = s_after[1];  // the item to load when a slot frees
+  auto map = [&](uint32_t v, uint32_t b, uint32_t c_tot, int c_sl) -> uint32_t {
+    return b + v < c_tot ? row_in(c_sl, b + v) : row_in(c_sl ^ 1, b + v - c_tot);
+  };
+  K k[R];
+  uint32_t rp[R];
+  uint32_t avail = tc - base + tn;  // rows mapped by the two loaded items
+#pragma unroll
+  for (int j = 0; j < R; ++j) {
+    const uint32_t v = lane_off + 32 * j;
+    rp[j] = v < avail ? map(v, base, tc, cur) : 0;
+    k[j] = v < avail ? __ldcs(keys + rp[j]) : (K)0;
+  }
+  bool prefetched = true;
+  while (avail > 0) {
+    const uint32_t take = avail < kChunk ? avail : kChunk;
+    if (!prefetched) {
+#pragma unroll
+      for (int j = 0; j < R; ++j) {
+        const uint32_t v = lane_off + 32 * j;
+        rp[j] = v < take ? map(v, base, tc, cur) : 0;
+        k[j] = v < take ? __ldcs(keys + rp[j]) : (K)0;
+      }
+    }
+    {
+      uint32_t r[R];
+      uint32_t act = 0;
+      uint32_t b[R];
+      uint64_t ks[R];
+#pragma unroll
+      for (int j = 0; j < R; ++j) {
+        r[j] = rp[j];
+        if (lane_off + 32 * j < take && in_range(t, k[j])) act |= 1u << j;
+        const uint64_t kb = key_u64<K>(k[j]);
+        b[j] = home_bucket(t, kb);
+        ks[j] = Ops::probe_key((uint64_t)(long long)k[j] - (uint64_t)t.kmin, kb, t.rbits);
+      }
+      // the next chunk's keys load while this chunk probes, when they lie in the loaded items
+      prefetched = avail - take >= kChunk;
+      if (prefetched) {
+#pragma unroll
+        for (int j = 0; j < R; ++j) {
+          rp[j] = map(take + lane_off + 32 * j, base, tc, cur);
+          k[j] = __ldcs(keys + rp[j]);
+        }
+      }
+      int32_t pos[R];
+      uint32_t hit = 0;
+#pragma unroll
+      for (int j = 0; j < R; ++j) pos[j] = 0;
+      for (uint32_t step = 0; act && step <= t.segmask; ++step) {
+        Bucket bk[R];
+#pragma unroll
+        for (int j = 0; j < R; ++j)
+          if (act >> j & 1u) bk[j] = load_bucket<true>(t.slots, b[j]);
+#pragma unroll
+        for (int j = 0; j < R; ++j) {
+          if (!(act >> j & 1u)) continue;
+          int32_t pj;
+          const bool m = Ops::match_distinct(bk[j], ks[j], kmask, t.rbits, pj);
+          if (m) {
+            pos[j] = pj;
+            hit |= 1u << j;
+          }
+          if (m || Ops::open(bk[j])) act &= ~(1u << j);
+          else b[j] = next_bucket(b[j], t.segmask);
+        }
+      }
+      int32_t prid[R], brid[R];
+      uint64_t pv[kDirectMaxProbePayload][R];
+      uint64_t bv[kDirectMaxBuildPayload][R];
+#pragma unroll
+      for (int j = 0; j < R; ++j) {
+        prid[j] = brid[j] = 0;
+#pragma unroll
+        for (int c = 0; c < kDirectMaxProbePayload; ++c) pv[c][j] = 0;
+#pragma unroll
+        for (int c = 0; c < kDirectMaxBuildPayload; ++c) bv[c][j] = 0;
+        if (!(hit >> j & 1u)) continue;
+        if (a.out_prid) prid[j] = a.prid_map ? __ldcs(a.prid_map + r[j]) : (int32_t)r[j];
+#pragma unroll
+        for (int c = 0; c < kDirectMaxProbePayload; ++c)
+          if (c < n_pin) pv[c][j] = ld_cs_w(a.pin[c], r[j], kFixed ? 8 : a.pin_w[c]);
+        if (use_rec) {
+          uint32_t wd[8];
+          load_rec(static_cast<const char*>(a.rec) + (size_t)(uint32_t)pos[j] * rec_stride, rec_stride, wd);
+          brid[j] = (int32_t)wd[0];
+#pragma unroll
+          for (int c = 0; c < kDirectMaxBuildPayload; ++c)
+            bv[c][j] = kFixed || a.rec_std ? ((uint64_t)wd[3 + 2 * c] << 32) | wd[2 + 2 * c]
+                                           : rec_word_field(wd, a.rec_off[c], a.bin_w[c]);
+        } else {
+          brid[j] = a.brid_map ? __ldg(reinterpret_cast<const int32_t*>(reinterpret_cast<const char*>(a.brid_map) +
+                                                                         (int64_t)pos[j] * a.brid_stride))
+                               : pos[j];
+#pragma unroll
+          for (int c = 0; c < kDirectMaxBuildPayload; ++c) {
+            if (c < n_bin) {
+              const int64_t i = a.bin_by_pos ? pos[j] : brid[j];
+              bv[c][j] = ld_nc_w(static_cast<const char*>(a.bin[c]) + i * a.bin_stride[c], a.bin_w[c]);
+            }
+          }
+        }
+      }
+      unsigned bal[R];
+      unsigned wtot = 0;
+#pragma unroll
+      for (int j = 0; j < R; ++j) {
+        bal[j] = __ballot_sync(kFullMask, (hit >> j) & 1u);
+        wtot += __popc(bal[j]);
+      }
+      if (lane == 0) s_wtot[warp] = wtot;
+      __syncthreads();
+      if (warp == 0) {
+        const unsigned v = lane < kDirectWarps ? s_wtot[lane] : 0u;
+        unsigned incl = v;
+#pragma unroll
+        for (int d = 1; d < kDirectWarps; d <<= 1) {
+          const unsigned o = __shfl_up_sync(kFullMask, incl, d);
+          if (lane >= d) incl += o;
+        }
+        const unsigned tot = __shfl_sync(kFullMask, incl, kDirectWarps - 1);
+        unsigned long long cb = 0;
+        if (lane == 0 && tot) cb = atomicAdd(a.d_count, (unsigned long long)tot);
+        cb = __shfl_sync(kFullMask, cb, 0);
+        if (lane < kDirectWarps) s_wbase[lane] = cb + (incl - v);
+      }
+      __syncthreads();
+      if (wtot != 0) {
+        uint32_t run = (uint32_t)s_wbase[warp];
+#pragma unroll
+        for (int j = 0; j < R; ++j) {
+          const uint32_t pj = run + __popc(bal[j] & below);
+          run += __popc(bal[j]);
+          if (!(hit >> j & 1u) || pj >= cap) continue;
+          if (a.out_prid) __stcs(a.out_prid + pj, prid[j]);
+          if (a.out_brid) __stcs(a.out_brid + pj, brid[j]);
+#pragma unroll
+          for (int c = 0; c < kDirectMaxProbePayload; ++c)
+            if (c < n_pin) st_cs_w(a.pout[c], pj, kFixed ? 8 : a.pin_w[c], pv[c][j]);
+#pragma unroll
+          for (int c = 0; c < kDirectMaxBuildPayload; ++c)
+            if (c < n_bin) st_cs_w(a.bout[c], pj, kFixed ? 8 : a.bin_w[c], bv[c][j]);
+        }
+      }
+    }
+    // advance past the rows taken; a finished item frees its slot for the next one
+    avail -= take;
+    base += take;
+    while (base >= tc && (tc != 0 || tn != 0 || w_after < n_items)) {
+      base -= tc;
+      cur ^= 1;
+      tc = tn;
+      if (warp == 0) load_item(cur ^ 1, w_after);
+      __syncthreads();
+      tn = (uint32_t)s_pre[cur ^ 1][kRunGroup];
+      w_after = s_after[cur ^ 1];
+    }
+    avail = (tc > base ? tc - base : 0) + tn;
+  }
+}
+
+// ------------------------------------------------------------------------------------------------
 // The same probe with its streaming inputs staged by the TMA engine. The probe rows of a tile
 // (keys, partition row ids, probe payloads: contiguous ranges) are bulk-copied into a 3-stage
 // shared-memory ring two tiles ahead of their use, so no lane waits on DRAM for them and no
@@ -654,6 +888,53 @@ bool probe_direct(const sj_table* t, const sj_column& p, const int64_t* d_n, con
     else launch_direct<int64_t, false>(t, p, d_n, a, rpl, mode, s);
   }
   return true;
+}
+
+bool probe_runs_ok(const sj_table* t, const GatherArgs& g) {
+  const sj_join_params& pr = t->params;
+  if (pr.probe_kernel == SJ_PROBE_KERNEL_STAGED || pr.probe_kernel == SJ_PROBE_KERNEL_DIRECT_TMA) return false;
+  if (pr.aggregation != SJ_AGG_AUTO && pr.aggregation != SJ_AGG_CTA) return false;
+  if (pr.rows_per_lane != 0 && pr.rows_per_lane != 2) return false;
+  DirectArgs a;
+  return direct_args(g, a);
+}
+
+template <typename K, bool WIDE, int SP, int SB>
+static void launch_runs_shape(const sj_table* t, const void* keys, const RunArgs& ra, const DirectArgs& a,
+                              cudaStream_t s) {
+  int resident = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, probe_runs_kernel<K, WIDE, SP, SB>, kDirectThreads, 0);
+  const int64_t items = (int64_t)ra.P * ((ra.n_tiles + kRunGroup - 1) / kRunGroup);
+  const int per_sm = std::min(std::max(1, resident), std::max(1, t->params.ctas_per_sm) * 256 / kDirectThreads);
+  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(items, (int64_t)sm_count(t->device) * per_sm));
+  probe_runs_kernel<K, WIDE, SP, SB><<<grid, kDirectThreads, 0, s>>>(table_dev(t), static_cast<const K*>(keys), ra, a);
+}
+
+template <typename K, bool WIDE>
+static void launch_runs(const sj_table* t, const void* keys, const RunArgs& ra, const DirectArgs& a, cudaStream_t s) {
+  int sp, sb;
+  fixed_shape(a, sp, sb);
+  if (sp == 1 && sb == 2) return launch_runs_shape<K, WIDE, 1, 2>(t, keys, ra, a, s);
+  if (sp == 0 && sb == 1) return launch_runs_shape<K, WIDE, 0, 1>(t, keys, ra, a, s);
+  launch_runs_shape<K, WIDE, -1, -1>(t, keys, ra, a, s);
+}
+
+void probe_runs(const sj_table* t, const void* keys, const RunArgs& ra, const GatherArgs& g, cudaStream_t s,
+                unsigned long long* tile_ctr) {
+  DirectArgs a;
+  direct_args(g, a);
+  cudaMemsetAsync(tile_ctr, 0, sizeof(unsigned long long), s);
+  a.tile_ctr = tile_ctr;
+  if (ra.n_tiles == 0) return;
+  KernelTimer timer("probe_direct", s);
+  const bool wide = t->slot_kind == SJ_SLOT_WIDE128;
+  if (t->key_type == SJ_INT32) {
+    if (wide) launch_runs<int32_t, true>(t, keys, ra, a, s);
+    else launch_runs<int32_t, false>(t, keys, ra, a, s);
+  } else {
+    if (wide) launch_runs<int64_t, true>(t, keys, ra, a, s);
+    else launch_runs<int64_t, false>(t, keys, ra, a, s);
+  }
 }
 
 }  // namespace sj

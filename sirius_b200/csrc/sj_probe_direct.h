@@ -33,6 +33,15 @@ struct DirectArgs {
   unsigned long long* tile_ctr;  // zeroed device word: dynamic tile order of CTA-reserving launches
 };
 
+// Partition runs of a tile-local partition (local_partition): rows of partition p in tile i are
+// [run_off[i * P + p], + run_cnt[i * P + p]).
+struct RunArgs {
+  const int32_t* run_off;
+  const int32_t* run_cnt;
+  uint32_t n_tiles;
+  uint32_t P;
+};
+
 // Fills `a` from a general gather description; false when the output shape needs the staged
 // kernel (NULL payloads, 1/2-byte payloads, too many columns, other record layouts).
 bool direct_args(const GatherArgs& g, DirectArgs& a);
@@ -43,5 +52,14 @@ bool direct_args(const GatherArgs& g, DirectArgs& a);
 // and a counter is needed, one is drawn from `alloc`.
 bool probe_direct(const sj_table* t, const sj_column& p, const int64_t* d_n, const GatherArgs& g, cudaStream_t s,
                   const Allocator& alloc, unsigned long long* tile_ctr);
+
+// True when probe_runs serves this gather (DIRECT write-out shape, CTA reservation).
+bool probe_runs_ok(const sj_table* t, const GatherArgs& g);
+
+// Probe of tile-local partition runs: `keys`, the partition row ids and payloads in `g` are the
+// partitioned arrays; work items (partition, group of 8 tiles) are taken partition-major from
+// `tile_ctr` (zeroed here). Requires probe_runs_ok.
+void probe_runs(const sj_table* t, const void* keys, const RunArgs& ra, const GatherArgs& g, cudaStream_t s,
+                unsigned long long* tile_ctr);
 
 }  // namespace sj

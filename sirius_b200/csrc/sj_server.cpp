@@ -122,9 +122,12 @@ static void size_request(const sj_server* S, SrvReq* r) {
   r->out_bytes = out;
   const int kw = T.t->key_type == SJ_INT32 ? 4 : 8;
   // a partitioned probe: partitioned keys + row ids + the partition histogram / offsets
+  // a partitioned probe: partitioned keys + row ids + the partition scratch (global offsets, or the
+  // run tables of the tile-local partition: 2 x int32 per tile and partition)
+  const size_t runs = 2 * a256((size_t)((n + kPartTileRows - 1) / kPartTileRows) * ((size_t)4 << T.t->pbits));
   r->scratch_bytes = 256 + (T.t->pbits > 0 && n >= kMinPartitionedProbe
-                               ? a256((size_t)n * kw) + a256((size_t)n * 4) +
-                                     partition_scratch_bytes(T.t->pbits, S->device) + 256
+                               ? a256((size_t)n * kw) + a256((size_t)n * 4) + 256 +
+                                     std::max(partition_scratch_bytes(T.t->pbits, S->device), runs)
                                : 0);
 }
 

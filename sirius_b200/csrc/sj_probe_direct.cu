@@ -262,12 +262,14 @@ __global__ void __launch_bounds__(kDirectThreads, (R <= 2 ? 1024 : R == 3 ? 768 
 }
 
 // ------------------------------------------------------------------------------------------------
-// The direct probe over tile-local partition runs. A work item is (partition p, 8 consecutive
-// tiles): its rows are the 8 runs of p in those tiles, concatenated; the CTA walks them in chunks of
-// 128 rows (lane l of warp w: chunk rows 64w + 32j + l) mapping each chunk row to its run through a
-// prefix of the 8 run lengths held in shared memory. Items are taken partition-major (all tiles of
-// partition 0 first) from the shared counter, so the CTAs sweep one partition's table rows at a
-// time. Output reservation: one atomicAdd per chunk (two CTA barriers), as in probe_direct_kernel.
+// The direct probe over tile-local partition runs. A work item is (partition p, 4 consecutive
+// tiles): its rows are the 4 runs of p in those tiles, concatenated. Items are taken partition-major
+// (all tiles of partition 0 first) from the shared counter, so the CTAs sweep one partition's table
+// rows at a time. A CTA keeps two item descriptors (run offsets and a prefix of run lengths in
+// shared memory) and walks their concatenation in full chunks of 128 rows (lane l of warp w: chunk
+// rows 64w + 32j + l), a chunk taking the tail of one item and the head of the next; a finished item
+// frees its slot for the next one. Output reservation: one atomicAdd per chunk (two CTA barriers),
+// as in probe_direct_kernel.
 // ------------------------------------------------------------------------------------------------
 constexpr int kRunGroup = 4;
 

@@ -360,14 +360,14 @@ __global__ void __launch_bounds__(kPartThreads, 3) part_scatter_fast_kernel(Part
     }
     unsigned tile_valid = 0;
     for (int w = 0; w < kPartThreads / 32; ++w) tile_valid += s_wsum[w];
-    if (LOCAL) {
+    __syncthreads();
+    if (LOCAL) {  // after the barrier: toff[p] is written by thread p / kBinsPerThread
       const int64_t ti = t0 / kTile;
       for (int p = tid; p < P; p += kPartThreads) {
         run_off[ti * P + p] = (int32_t)(t0 + toff[p]);
         run_cnt[ti * P + p] = (int32_t)tcnt[p];
       }
     }
-    __syncthreads();
     // 3. counting-sort the tile into shared memory (payloads straight to their sorted slot, with
     //    each row's output position, so the write-out reads nothing per partition)
 #pragma unroll

@@ -58,6 +58,9 @@ def parse():
     ap.add_argument("--aggregation", type=int, default=0)
     ap.add_argument("--probe-kernel", type=int, default=0, help="0 auto, 1 staged write-out, 2 direct write-out")
     ap.add_argument("--rows-per-lane", type=int, default=0)
+    ap.add_argument("--probe-partition-mb", type=int, default=0,
+                    help="table MB per probe partition of the partitioned probe (0 = default)")
+    ap.add_argument("--table-l2", type=int, default=0, help="L2 priority of table loads: 0 auto, 1 normal, 2 evict_last")
     ap.add_argument("--ctas-per-sm", type=int, default=0)
     ap.add_argument("--workload", default="large", choices=["large", "small", "skewed", "batched", "served"])
     ap.add_argument("--autotune", action="store_true", help="batched: choose launch parameters by the autotuner")
@@ -265,7 +268,8 @@ def run_sj(args):
         ev0.record()
         tb = J.HashTable(bk, attach=bp, partition_bits=args.partition_bits, aggregation=args.aggregation,
                          probe_kernel=args.probe_kernel, rows_per_lane=args.rows_per_lane,
-                         ctas_per_sm=args.ctas_per_sm, load_factor=args.load_factor or 0.5)
+                         ctas_per_sm=args.ctas_per_sm, load_factor=args.load_factor or 0.5,
+                         probe_partition_mb=args.probe_partition_mb, table_l2_priority=args.table_l2)
         ev1.record()
         torch.cuda.synchronize()
         t_build.append(ev0.elapsed_time(ev1))
@@ -341,7 +345,8 @@ def run_sj(args):
             for d, h in zip(d_bp + d_pp, h_bp + h_pp):
                 d.copy_(h, non_blocking=True)
             with J.HashTable(d_bk, attach=d_bp, partition_bits=args.partition_bits, probe_kernel=args.probe_kernel,
-                             rows_per_lane=args.rows_per_lane) as tt:
+                             rows_per_lane=args.rows_per_lane, probe_partition_mb=args.probe_partition_mb,
+                             table_l2_priority=args.table_l2) as tt:
                 tt.probe_gather(d_pk, None, d_pp, attached=True, capacity=args.n_probe, out=out, d_count=d_count,
                                 sync=False)
                 srcs = [out.probe_rid, out.build_rid] + out.probe_payload + out.build_payload
@@ -410,7 +415,8 @@ def run_sj(args):
                        "table": {"layout": "DISTINCT" if info.layout == 1 else "GROUPED",
                                  "slot": "PACKED64" if info.slot_kind == 0 else "WIDE128",
                                  "slots": int(info.num_slots), "rid_bits": int(info.rid_bits),
-                                 "bytes": int(info.device_bytes), "partition_bits": int(info.partition_bits)},
+                                 "bytes": int(info.device_bytes), "partition_bits": int(info.partition_bits),
+                                 "probe_partition_mb": args.probe_partition_mb or 48, "table_l2": args.table_l2},
                        "t_build_ms": round(min(t_build), 3)},
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4), "traffic": traffic,

@@ -152,6 +152,13 @@ typedef enum sj_probe_kernel {
   SJ_PROBE_KERNEL_DIRECT_TMA = 3
 } sj_probe_kernel;
 
+/* L2 eviction priority of the table loads of a probe (PTX createpolicy / L2::cache_hint). */
+typedef enum sj_l2_priority {
+  SJ_L2_AUTO = 0,       /* the default below */
+  SJ_L2_NORMAL = 1,     /* plain loads */
+  SJ_L2_EVICT_LAST = 2  /* table lines evicted after the probe stream's */
+} sj_l2_priority;
+
 typedef struct sj_join_params {
   int32_t layout;           /* sj_layout */
   int32_t null_equality;    /* sj_null_equality */
@@ -166,7 +173,11 @@ typedef struct sj_join_params {
   int32_t aggregation;      /* sj_aggregation: how probe matches reserve output positions */
   int32_t probe_kernel;     /* sj_probe_kernel: write-out of DISTINCT probes; default AUTO */
   int32_t rows_per_lane;    /* probe rows per lane and tile of the direct kernel: 2 or 4; 0 = 2 */
-  int32_t reserved[5];
+  int32_t probe_partition_mb; /* partitioned probe: table megabytes per probe partition (the part
+                                 of the table one sweep keeps in L2); 0 = default (48) */
+  int32_t table_l2_priority;  /* sj_l2_priority of the table's slot and record loads in the
+                                 direct probe kernels */
+  int32_t reserved[3];
 } sj_join_params;
 
 typedef struct sj_table sj_table;

@@ -25,6 +25,7 @@ SJ_AGG_AUTO, SJ_AGG_WARP, SJ_AGG_CTA, SJ_AGG_WARP_DYNAMIC = 0, 1, 2, 3
 SJ_JOIN_INNER, SJ_JOIN_LEFT, SJ_JOIN_SEMI, SJ_JOIN_ANTI, SJ_JOIN_MARK, SJ_JOIN_FULL = range(6)
 SJ_NO_ROW = -(1 << 31)
 SJ_PROBE_KERNEL_AUTO, SJ_PROBE_KERNEL_STAGED, SJ_PROBE_KERNEL_DIRECT, SJ_PROBE_KERNEL_DIRECT_TMA = 0, 1, 2, 3
+SJ_L2_AUTO, SJ_L2_NORMAL, SJ_L2_EVICT_LAST = 0, 1, 2
 
 
 class SjColumn(Structure):
@@ -48,7 +49,8 @@ class SjJoinParams(Structure):
     _fields_ = [("layout", c_int32), ("null_equality", c_int32), ("load_factor", c_float),
                 ("block_size", c_int32), ("group_width", c_int32), ("partition_bits", c_int32),
                 ("force_wide", c_int32), ("ctas_per_sm", c_int32), ("aggregation", c_int32),
-                ("probe_kernel", c_int32), ("rows_per_lane", c_int32), ("reserved", c_int32 * 5)]
+                ("probe_kernel", c_int32), ("rows_per_lane", c_int32), ("probe_partition_mb", c_int32),
+                ("table_l2_priority", c_int32), ("reserved", c_int32 * 3)]
 
 
 class SjTableInfo(Structure):

@@ -170,6 +170,8 @@ static sj_join_params resolve(const sj_join_params* p) {
   r.aggregation = p->aggregation;
   r.probe_kernel = p->probe_kernel;
   r.rows_per_lane = p->rows_per_lane;
+  r.probe_partition_mb = p->probe_partition_mb;
+  r.table_l2_priority = p->table_l2_priority;
   return r;
 }
 

@@ -419,6 +419,10 @@ sj_status build_table(const sj_column& keys, const sj_column* payload, int32_t n
     return set_error(SJ_ERR_INVALID, "unknown probe_kernel");
   if (p.rows_per_lane != 0 && (p.rows_per_lane < 2 || p.rows_per_lane > 4))
     return set_error(SJ_ERR_INVALID, "rows_per_lane must be 0 (default), 2, 3 or 4");
+  if (p.probe_partition_mb < 0 || p.probe_partition_mb > 65536)
+    return set_error(SJ_ERR_INVALID, "probe_partition_mb must be in [0, 65536]");
+  if (p.table_l2_priority < SJ_L2_AUTO || p.table_l2_priority > SJ_L2_EVICT_LAST)
+    return set_error(SJ_ERR_INVALID, "unknown table_l2_priority");
   if (n_payload < 0 || n_payload > kMaxPayload || (n_payload > 0 && payload == nullptr))
     return set_error(SJ_ERR_INVALID, "at most 8 attached payload columns");
   for (int c = 0; c < n_payload; ++c) {

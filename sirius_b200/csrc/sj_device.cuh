@@ -99,6 +99,24 @@ __device__ __forceinline__ Bucket load_bucket(const void* slots, uint32_t b) {
   return r;
 }
 
+// L2 policy for table loads that should outlive the probe stream's lines in L2 (PTX createpolicy:
+// every access through it is marked evict_last).
+__device__ __forceinline__ uint64_t l2_policy_evict_last() {
+  uint64_t pol;
+  asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
+  return pol;
+}
+
+// load_bucket<true> with an L2 cache policy.
+__device__ __forceinline__ Bucket load_bucket_hint(const void* slots, uint32_t b, uint64_t pol) {
+  Bucket r;
+  const unsigned long long* p = reinterpret_cast<const unsigned long long*>(slots) + (size_t)b * 4;
+  asm("ld.global.nc.L2::cache_hint.v4.u64 {%0, %1, %2, %3}, [%4], %5;"
+      : "=l"(r.a[0]), "=l"(r.a[1]), "=l"(r.a[2]), "=l"(r.a[3])
+      : "l"(p), "l"(pol));
+  return r;
+}
+
 // A row-store record of up to 32 bytes in one load (4, 8, 16 or 32 bytes, naturally aligned).
 struct Record {
   uint32_t w[8];

@@ -764,15 +764,16 @@ static size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
 // the table's partition bits, then stream the partitioned arrays through the probe kernel, so
 // each partition's probes hit its L2-resident table segment and attached payload rows.
 // Probe-side radix bits: the coarsest prefix of the table's partition bits whose share of the
-// table footprint (slots + position map + attached payloads) stays under 48 MB of L2. A coarse
+// table footprint (slots + position map + attached payloads) stays under 48 MB of L2 (or the
+// table's probe_partition_mb). A coarse
 // probe partition covers 2^(table bits - probe bits) contiguous table segments, and fewer
 // partitions mean longer contiguous runs in the scatter (16M-row table, 768 MB: 12 MB shares made
 // the probe 2 % faster and the scatter 15 % slower than 48 MB shares; 24 MB was in between).
 static int probe_partition_bits(const sj_table* t) {
   size_t fp = t->slots_bytes + t->arow_bytes;
-  const size_t kShare = 48ull << 20;
+  const size_t share = (size_t)(t->params.probe_partition_mb > 0 ? t->params.probe_partition_mb : 48) << 20;
   int b = 1;
-  while (b < t->pbits && (fp >> b) > kShare) ++b;
+  while (b < t->pbits && (fp >> b) > share) ++b;
   return std::min(b, t->pbits);
 }
 

@@ -19,6 +19,7 @@
 #include "sj_bulk.cuh"
 #include "sj_device.cuh"
 #include "sj_internal.h"
+#include "sj_partition.cuh"
 #include "sj_probe_direct.h"
 
 namespace sj {
@@ -39,6 +40,23 @@ __device__ __forceinline__ uint64_t ld_nc_w(const void* a, int w) {
 __device__ __forceinline__ void st_cs_w(void* base, int64_t i, int w, uint64_t v) {
   if (w == 8) __stcs(reinterpret_cast<unsigned long long*>(base) + i, (unsigned long long)v);
   else __stcs(reinterpret_cast<unsigned int*>(base) + i, (unsigned int)v);
+}
+
+// One row-store record of 8, 16 or 32 bytes (the stride) in one load, under L2 policy `pol`.
+__device__ __forceinline__ void load_rec_hint(const void* p, int stride, uint32_t (&w)[8], uint64_t pol) {
+  if (stride == 32) {
+    asm("ld.global.nc.L2::cache_hint.v8.u32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8], %9;"
+        : "=r"(w[0]), "=r"(w[1]), "=r"(w[2]), "=r"(w[3]), "=r"(w[4]), "=r"(w[5]), "=r"(w[6]), "=r"(w[7])
+        : "l"(p), "l"(pol));
+  } else if (stride == 16) {
+    asm("ld.global.nc.L2::cache_hint.v4.u32 {%0, %1, %2, %3}, [%4], %5;"
+        : "=r"(w[0]), "=r"(w[1]), "=r"(w[2]), "=r"(w[3])
+        : "l"(p), "l"(pol));
+    w[4] = w[5] = w[6] = w[7] = 0;
+  } else {
+    asm("ld.global.nc.L2::cache_hint.v2.u32 {%0, %1}, [%2], %3;" : "=r"(w[0]), "=r"(w[1]) : "l"(p), "l"(pol));
+    w[2] = w[3] = w[4] = w[5] = w[6] = w[7] = 0;
+  }
 }
 
 // One row-store record of 8, 16 or 32 bytes (the stride) in one load.
@@ -81,6 +99,7 @@ __global__ void __launch_bounds__(kDirectThreads, (R <= 2 ? 1024 : R == 3 ? 768 
     probe_direct_kernel(TableDev t, const K* __restrict__ keys, const uint32_t* __restrict__ kv, int64_t kvoff,
                         int64_t n_host, const int64_t* d_n, DirectArgs a) {
   using Ops = SlotOps<WIDE>;
+  const uint64_t pol = a.l2_last ? l2_policy_evict_last() : 0ull;  // table loads' L2 policy
   constexpr bool kFixed = SP >= 0;
   const int n_pin = kFixed ? SP : a.n_pin;
   const int n_bin = kFixed ? SB : a.n_bin;
@@ -144,7 +163,7 @@ __global__ void __launch_bounds__(kDirectThreads, (R <= 2 ? 1024 : R == 3 ? 768 
       Bucket bk[R];
 #pragma unroll
       for (int j = 0; j < R; ++j)
-        if (act >> j & 1u) bk[j] = load_bucket<true>(t.slots, b[j]);
+        if (act >> j & 1u) bk[j] = a.l2_last ? load_bucket_hint(t.slots, b[j], pol) : load_bucket<true>(t.slots, b[j]);
 #pragma unroll
       for (int j = 0; j < R; ++j) {
         if (!(act >> j & 1u)) continue;
@@ -178,7 +197,9 @@ __global__ void __launch_bounds__(kDirectThreads, (R <= 2 ? 1024 : R == 3 ? 768 
         if (c < n_pin) pv[c][j] = ld_cs_w(a.pin[c], r, kFixed ? 8 : a.pin_w[c]);
       if (use_rec) {
         uint32_t w[8];
-        load_rec(static_cast<const char*>(a.rec) + (size_t)(uint32_t)pos[j] * rec_stride, rec_stride, w);
+        const char* recp = static_cast<const char*>(a.rec) + (size_t)(uint32_t)pos[j] * rec_stride;
+        if (a.l2_last) load_rec_hint(recp, rec_stride, w, pol);
+        else load_rec(recp, rec_stride, w);
         brid[j] = (int32_t)w[0];
 #pragma unroll
         for (int c = 0; c < kDirectMaxBuildPayload; ++c)
@@ -271,12 +292,14 @@ __global__ void __launch_bounds__(kDirectThreads, (R <= 2 ? 1024 : R == 3 ? 768 
 // frees its slot for the next one. Output reservation: one atomicAdd per chunk (two CTA barriers),
 // as in probe_direct_kernel.
 // ------------------------------------------------------------------------------------------------
-constexpr int kRunGroup = 4;
+constexpr int kMaxRunGroup = 16;
+constexpr int kRunItemRows = 512;
 
 template <typename K, bool WIDE, int SP, int SB>
 __global__ void __launch_bounds__(kDirectThreads, 1024 / kDirectThreads)
     probe_runs_kernel(TableDev t, const K* __restrict__ keys, RunArgs ra, DirectArgs a) {
   using Ops = SlotOps<WIDE>;
+  const uint64_t pol = a.l2_last ? l2_policy_evict_last() : 0ull;  // table loads' L2 policy
   constexpr int R = 2;
   constexpr bool kFixed = SP >= 0;
   const int n_pin = kFixed ? SP : a.n_pin;
@@ -288,8 +311,8 @@ __global__ void __launch_bounds__(kDirectThreads, 1024 / kDirectThreads)
   __shared__ unsigned long long s_wbase[kDirectWarps];
   // two item descriptors: the item being walked and the next one, so a chunk can take the tail
   // of one item and the head of the next (chunks stay full)
-  __shared__ int32_t s_off[2][kRunGroup];
-  __shared__ int32_t s_pre[2][kRunGroup + 1];
+  __shared__ int32_t s_off[2][kMaxRunGroup];
+  __shared__ int32_t s_pre[2][kMaxRunGroup + 1];  // entries past the item's tiles hold its total
   __shared__ uint32_t s_after[2];  // the item to load after the one in the slot
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
@@ -297,24 +320,25 @@ __global__ void __launch_bounds__(kDirectThreads, 1024 / kDirectThreads)
   const uint32_t cap = (uint32_t)(a.capacity < (int64_t)INT32_MAX ? a.capacity : (int64_t)INT32_MAX);
   const uint64_t kmask = ~((1ull << t.rbits) - 1);
   const uint32_t lane_off = (uint32_t)warp * (32 * R) + lane;
-  const uint32_t n_groups = (ra.n_tiles + kRunGroup - 1) / kRunGroup;
+  const uint32_t G = ra.group;
+  const uint32_t n_groups = (ra.n_tiles + G - 1) / G;
   const uint32_t n_items = ra.P * n_groups;
   // warp 0: descriptor of item w into slot `sl` (w >= n_items: an empty item) and the index of the
   // item after it (taken from the shared counter) into s_after[sl]
   auto load_item = [&](int sl, uint32_t w) {
     const bool in = w < n_items;
     const uint32_t p = in ? w / n_groups : 0, g = in ? w - p * n_groups : 0;
-    const uint32_t ti = g * kRunGroup + lane;
-    const bool ok = in && lane < kRunGroup && ti < ra.n_tiles;
+    const uint32_t ti = g * G + lane;
+    const bool ok = in && (uint32_t)lane < G && ti < ra.n_tiles;
     const int32_t cnt = ok ? __ldg(ra.run_cnt + (size_t)ti * ra.P + p) : 0;
-    if (lane < kRunGroup) s_off[sl][lane] = ok ? __ldg(ra.run_off + (size_t)ti * ra.P + p) : 0;
+    if (lane < kMaxRunGroup) s_off[sl][lane] = ok ? __ldg(ra.run_off + (size_t)ti * ra.P + p) : 0;
     int32_t incl = cnt;
 #pragma unroll
     for (int d = 1; d < 32; d <<= 1) {
       const int32_t o = __shfl_up_sync(kFullMask, incl, d);
       if (lane >= d) incl += o;
     }
-    if (lane < kRunGroup) s_pre[sl][lane + 1] = incl;
+    if (lane < kMaxRunGroup) s_pre[sl][lane + 1] = incl;
     if (lane == 0) {
       s_pre[sl][0] = 0;
       s_after[sl] = in ? gridDim.x + (uint32_t)atomicAdd(a.tile_ctr, 1ull) : w;
@@ -323,8 +347,7 @@ __global__ void __launch_bounds__(kDirectThreads, 1024 / kDirectThreads)
   // chunk row v of the concatenation (slot cur from `base` on, then slot cur ^ 1) -> array position
   auto row_in = [&](int sl, uint32_t v) -> uint32_t {
     int q = 0;
-#pragma unroll
-    for (int step = kRunGroup / 2; step > 0; step >>= 1)
+    for (uint32_t step = G / 2; step > 0; step >>= 1)
       if ((uint32_t)s_pre[sl][q + step] <= v) q += step;
     return (uint32_t)s_off[sl][q] + (v - (uint32_t)s_pre[sl][q]);
   };
@@ -334,7 +357,7 @@ __global__ void __launch_bounds__(kDirectThreads, 1024 / kDirectThreads)
   __syncthreads();
   int cur = 0;
   uint32_t base = 0;  // rows of item `cur` already taken
-  uint32_t tc = (uint32_t)s_pre[0][kRunGroup], tn = (uint32_t)s_pre[1][kRunGroup];
+  uint32_t tc = (uint32_t)s_pre[0][kMaxRunGroup], tn = (uint32_t)s_pre[1][kMaxRunGroup];
   uint32_t w_after = s_after[1];  // the item to load when a slot frees
   auto map = [&](uint32_t v, uint32_t b, uint32_t c_tot, int c_sl) -> uint32_t {
     return b + v < c_tot ? row_in(c_sl, b + v) : row_in(c_sl ^ 1, b + v - c_tot);
@@ -389,7 +412,7 @@ __global__ void __launch_bounds__(kDirectThreads, 1024 / kDirectThreads)
         Bucket bk[R];
 #pragma unroll
         for (int j = 0; j < R; ++j)
-          if (act >> j & 1u) bk[j] = load_bucket<true>(t.slots, b[j]);
+          if (act >> j & 1u) bk[j] = a.l2_last ? load_bucket_hint(t.slots, b[j], pol) : load_bucket<true>(t.slots, b[j]);
 #pragma unroll
         for (int j = 0; j < R; ++j) {
           if (!(act >> j & 1u)) continue;
@@ -420,7 +443,9 @@ __global__ void __launch_bounds__(kDirectThreads, 1024 / kDirectThreads)
           if (c < n_pin) pv[c][j] = ld_cs_w(a.pin[c], r[j], kFixed ? 8 : a.pin_w[c]);
         if (use_rec) {
           uint32_t wd[8];
-          load_rec(static_cast<const char*>(a.rec) + (size_t)(uint32_t)pos[j] * rec_stride, rec_stride, wd);
+          const char* recp = static_cast<const char*>(a.rec) + (size_t)(uint32_t)pos[j] * rec_stride;
+          if (a.l2_last) load_rec_hint(recp, rec_stride, wd, pol);
+          else load_rec(recp, rec_stride, wd);
           brid[j] = (int32_t)wd[0];
 #pragma unroll
           for (int c = 0; c < kDirectMaxBuildPayload; ++c)
@@ -490,7 +515,7 @@ __global__ void __launch_bounds__(kDirectThreads, 1024 / kDirectThreads)
       tc = tn;
       if (warp == 0) load_item(cur ^ 1, w_after);
       __syncthreads();
-      tn = (uint32_t)s_pre[cur ^ 1][kRunGroup];
+      tn = (uint32_t)s_pre[cur ^ 1][kMaxRunGroup];
       w_after = s_after[cur ^ 1];
     }
     avail = (tc > base ? tc - base : 0) + tn;
@@ -536,6 +561,7 @@ __global__ void __launch_bounds__(kDirectThreads, 4)
     probe_tma_kernel(TableDev t, const K* __restrict__ keys, const uint32_t* __restrict__ kv, int64_t kvoff,
                      int64_t n_host, const int64_t* d_n, DirectArgs a, TmaStage st) {
   using Ops = SlotOps<WIDE>;
+  const uint64_t pol = a.l2_last ? l2_policy_evict_last() : 0ull;  // table loads' L2 policy
   constexpr int R = kTmaR;
   extern __shared__ __align__(128) unsigned char s_ring[];
   __shared__ __align__(8) uint64_t s_bar[kTmaStages];
@@ -612,7 +638,7 @@ __global__ void __launch_bounds__(kDirectThreads, 4)
       Bucket bk[R];
 #pragma unroll
       for (int j = 0; j < R; ++j)
-        if (act >> j & 1u) bk[j] = load_bucket<true>(t.slots, b[j]);
+        if (act >> j & 1u) bk[j] = a.l2_last ? load_bucket_hint(t.slots, b[j], pol) : load_bucket<true>(t.slots, b[j]);
 #pragma unroll
       for (int j = 0; j < R; ++j) {
         if (!(act >> j & 1u)) continue;
@@ -862,6 +888,7 @@ bool probe_direct(const sj_table* t, const sj_column& p, const int64_t* d_n, con
     if (cudaMemsetAsync(tile_ctr, 0, sizeof(unsigned long long), s) != cudaSuccess) return false;
   }
   a.tile_ctr = tile_ctr;
+  a.l2_last = pr.table_l2_priority == SJ_L2_EVICT_LAST;
   // AUTO takes the plain-load kernel: on the large 1:1 join the TMA ring's per-tile CTA barriers
   // cost more than the DRAM latency it hides (measured 1.96 vs 1.73 ms per 64M probe rows)
   bool tma = pr.probe_kernel == SJ_PROBE_KERNEL_DIRECT_TMA && (!a.rec || a.rec_std);
@@ -906,7 +933,7 @@ static void launch_runs_shape(const sj_table* t, const void* keys, const RunArgs
                               cudaStream_t s) {
   int resident = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, probe_runs_kernel<K, WIDE, SP, SB>, kDirectThreads, 0);
-  const int64_t items = (int64_t)ra.P * ((ra.n_tiles + kRunGroup - 1) / kRunGroup);
+  const int64_t items = (int64_t)ra.P * ((ra.n_tiles + ra.group - 1) / ra.group);
   const int per_sm = std::min(std::max(1, resident), std::max(1, t->params.ctas_per_sm) * 256 / kDirectThreads);
   const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(items, (int64_t)sm_count(t->device) * per_sm));
   probe_runs_kernel<K, WIDE, SP, SB><<<grid, kDirectThreads, 0, s>>>(table_dev(t), static_cast<const K*>(keys), ra, a);
@@ -921,12 +948,20 @@ static void launch_runs(const sj_table* t, const void* keys, const RunArgs& ra, 
   launch_runs_shape<K, WIDE, -1, -1>(t, keys, ra, a, s);
 }
 
-void probe_runs(const sj_table* t, const void* keys, const RunArgs& ra, const GatherArgs& g, cudaStream_t s,
+void probe_runs(const sj_table* t, const void* keys, const RunArgs& ra_in, const GatherArgs& g, cudaStream_t s,
                 unsigned long long* tile_ctr) {
+  // Tiles per work item: about kRunItemRows rows per item (a tile holds kPartTileRows / P rows of
+  // a partition). The CTAs walk some thousand items at once; short items keep those rows a small
+  // part of one partition's rows, so the table rows in use stay about one partition's share.
+  RunArgs ra = ra_in;
+  ra.group = 1;
+  while (ra.group < (uint32_t)kMaxRunGroup && (uint64_t)ra.group * kPartTileRows < (uint64_t)kRunItemRows * ra.P)
+    ra.group <<= 1;
   DirectArgs a;
   direct_args(g, a);
   cudaMemsetAsync(tile_ctr, 0, sizeof(unsigned long long), s);
   a.tile_ctr = tile_ctr;
+  a.l2_last = t->params.table_l2_priority == SJ_L2_EVICT_LAST;
   if (ra.n_tiles == 0) return;
   KernelTimer timer("probe_direct", s);
   const bool wide = t->slot_kind == SJ_SLOT_WIDE128;

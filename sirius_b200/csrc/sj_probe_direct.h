@@ -31,6 +31,7 @@ struct DirectArgs {
   int64_t capacity;
   unsigned long long* d_count;
   unsigned long long* tile_ctr;  // zeroed device word: dynamic tile order of CTA-reserving launches
+  int32_t l2_last;               // table slot and record loads marked L2 evict_last
 };
 
 // Partition runs of a tile-local partition (local_partition): rows of partition p in tile i are
@@ -40,6 +41,7 @@ struct RunArgs {
   const int32_t* run_cnt;
   uint32_t n_tiles;
   uint32_t P;
+  uint32_t group;  // tiles per work item (a power of two <= 16); set by probe_runs
 };
 
 // Fills `a` from a general gather description; false when the output shape needs the staged
@@ -57,7 +59,7 @@ bool probe_direct(const sj_table* t, const sj_column& p, const int64_t* d_n, con
 bool probe_runs_ok(const sj_table* t, const GatherArgs& g);
 
 // Probe of tile-local partition runs: `keys`, the partition row ids and payloads in `g` are the
-// partitioned arrays; work items (partition, group of 8 tiles) are taken partition-major from
+// partitioned arrays; work items (partition, group of tiles) are taken partition-major from
 // `tile_ctr` (zeroed here). Requires probe_runs_ok.
 void probe_runs(const sj_table* t, const void* keys, const RunArgs& ra, const GatherArgs& g, cudaStream_t s,
                 unsigned long long* tile_ctr);

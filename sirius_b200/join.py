@@ -141,6 +141,7 @@ class HashTable:
                  load_factor: float = 0.5, partition_bits: int = 0, force_wide: bool = False,
                  ctas_per_sm: int = 0, aggregation: int = L.SJ_AGG_AUTO,
                  probe_kernel: int = L.SJ_PROBE_KERNEL_AUTO, rows_per_lane: int = 0,
+                 probe_partition_mb: int = 0, table_l2_priority: int = L.SJ_L2_AUTO,
                  stream: Optional[torch.cuda.Stream] = None):
         """Build the table. ``attach``: build payload columns (tensor or (tensor, validity)) the
         table copies in its own position order (sj_build_ex); gather them with
@@ -151,7 +152,8 @@ class HashTable:
         self.params = L.default_params(layout=layout, null_equality=null_equality, load_factor=load_factor,
                                        partition_bits=partition_bits, force_wide=int(force_wide),
                                        aggregation=aggregation, probe_kernel=probe_kernel,
-                                       rows_per_lane=rows_per_lane)
+                                       rows_per_lane=rows_per_lane, probe_partition_mb=probe_partition_mb,
+                                       table_l2_priority=table_l2_priority)
         if ctas_per_sm:
             self.params.ctas_per_sm = ctas_per_sm
         col, nkeys, first = _keys(keys, validity)

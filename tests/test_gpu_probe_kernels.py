@@ -103,3 +103,24 @@ def test_tma_kernel_takes_unaligned_probe_columns(cuda):
     got = [out.probe_rid.cpu().numpy(), out.build_rid.cpu().numpy()] + \
         [c.cpu().numpy() for c in out.probe_payload] + [c.cpu().numpy() for c in out.build_payload]
     assert_same_rows(got, oracle_join(inp))
+
+
+@pytest.mark.parametrize("l2", [L.SJ_L2_NORMAL, L.SJ_L2_EVICT_LAST])
+@pytest.mark.parametrize("share_mb", [0, 1])
+def test_table_l2_priority_and_probe_partition_share(cuda, l2, share_mb):
+    """The L2 policy of the table loads and the probe's partition share change where lines live
+    and how many probe partitions there are, never the result; wide slots cover the 128-bit loads."""
+    for full_range in (False, True):
+        inp = _input(16, np.int64, 400_001, 1_500_007, full_range=full_range)
+        for attach in (False, True):
+            got = _run(inp, cuda, L.SJ_PROBE_KERNEL_AUTO, attach, partition_bits=6, table_l2_priority=l2,
+                       probe_partition_mb=share_mb)
+            assert_same_rows(got, oracle_join(inp))
+
+
+def test_l2_priority_and_share_are_validated(cuda):
+    k = dev_t(np.arange(1000, dtype=np.int64), cuda)
+    with pytest.raises(L.SjError):
+        J.HashTable(k, table_l2_priority=3)
+    with pytest.raises(L.SjError):
+        J.HashTable(k, probe_partition_mb=-1)

@@ -470,6 +470,30 @@ SJ_EXPORT sj_status sj_server_release(sj_server* server, uint64_t request_id);
 /* Stop the worker after the queued and in-flight requests finish and free everything. */
 SJ_EXPORT sj_status sj_server_destroy(sj_server* server);
 
+/* The one-shot INNER join of sj_inner_join with every column in HOST memory (pinned memory for
+ * full speed): the operator's whole join when its batches live in host memory, as the reference's
+ * memory spaces allow (batches are moved to the device before a GPU operator runs, and results
+ * are read back after it; src/op/sirius_physical_hash_join.cpp:1527-1955 runs in between).
+ * The build side is copied to the device and built with its payloads attached (sj_build_ex). The
+ * probe side streams through in chunks of `chunk_rows` rows (0 = 8M; rounded up to a multiple of
+ * 32). Chunk i+2 uploads on one copy stream while chunk i is probed on `stream` and chunk i-1's
+ * output downloads on another copy stream, so host-to-device and device-to-host traffic overlap.
+ * The output has the same columns and meaning as sj_inner_join, with probe row ids of the whole
+ * probe. It is written to host buffers in chunk order, and rows past `capacity` are not written.
+ * *out_count (a host pointer) receives the full match count.
+ * Key columns may carry NULLs (validity at any offset). Payload columns with NULLs are refused
+ * with SJ_ERR_INVALID. Device memory comes from `alloc`: the build copy, then the table, plus two
+ * input and two output chunk slots. Returns when every output row is on the host. */
+SJ_EXPORT sj_status sj_inner_join_host(const sj_column* build_keys, const sj_column* probe_keys,
+                                       int32_t num_keys, const sj_column* probe_payload,
+                                       int32_t num_probe_payload, const sj_column* build_payload,
+                                       int32_t num_build_payload, int32_t* out_probe_rid,
+                                       int32_t* out_build_rid,
+                                       const sj_mut_column* out_probe_payload,
+                                       const sj_mut_column* out_build_payload, int64_t capacity,
+                                       int64_t chunk_rows, const sj_join_params* params,
+                                       const sj_alloc* alloc, sj_stream_t stream, int64_t* out_count);
+
 /* The one-shot INNER join of sj_inner_join for callers that cannot allocate device memory: code
  * held to a device-memory reservation that is already fully committed (an allocation attempt
  * there would be refused and rescheduled as out-of-memory), latency-critical host threads that

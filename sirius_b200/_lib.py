@@ -104,6 +104,9 @@ SIGNATURES = {
     "sj_inner_join": (c_int32, [_P(SjColumn), _P(SjColumn), c_int32, _P(SjColumn), c_int32, _P(SjColumn), c_int32,
                                 c_void_p, c_void_p, _P(SjMutColumn), _P(SjMutColumn), c_int64, _P(SjJoinParams),
                                 _P(SjAlloc), c_void_p, c_void_p]),
+    "sj_inner_join_host": (c_int32, [_P(SjColumn), _P(SjColumn), c_int32, _P(SjColumn), c_int32, _P(SjColumn),
+                                     c_int32, c_void_p, c_void_p, _P(SjMutColumn), _P(SjMutColumn), c_int64, c_int64,
+                                     _P(SjJoinParams), _P(SjAlloc), c_void_p, _P(c_int64)]),
     "sj_inner_join_noalloc": (c_int32, [_P(SjColumn), _P(SjColumn), c_int32, _P(SjColumn), c_int32, _P(SjColumn),
                                         c_int32, c_void_p, c_void_p, _P(SjMutColumn), _P(SjMutColumn), c_int64,
                                         _P(SjJoinParams), c_void_p, c_void_p]),

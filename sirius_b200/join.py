@@ -329,6 +329,69 @@ def inner_join(build_keys, probe_keys, build_validity=None, probe_validity=None,
                               stream=stream).trimmed()
 
 
+def _host_column(data: torch.Tensor, validity: Optional[torch.Tensor] = None) -> L.SjColumn:
+    """A column in host memory for sj_inner_join_host (pinned memory lets its copies overlap)."""
+    if data.dim() != 1 or not data.is_contiguous() or data.is_cuda:
+        raise ValueError("host columns must be contiguous 1-D CPU tensors")
+    if validity is not None and (validity.is_cuda or validity.dtype not in (torch.int32, torch.uint32)):
+        raise ValueError("host validity must be a CPU int32/uint32 tensor of bitmask words")
+    col = L.SjColumn()
+    col.data = data.data_ptr() if data.numel() else None
+    col.validity = validity.data_ptr() if validity is not None else None
+    col.validity_offset = 0
+    col.num_rows = data.numel()
+    col.type = sj_type(data.dtype)
+    return col
+
+
+def inner_join_host(build_keys, probe_keys, build_validity=None, probe_validity=None, probe_payload=(),
+                    build_payload=(), *, capacity: Optional[int] = None, out: Optional[JoinOutput] = None,
+                    chunk_rows: int = 0, stream: Optional[torch.cuda.Stream] = None, **table_kwargs) -> JoinOutput:
+    """One-shot INNER join of host (CPU) tensors into host tensors (sj_inner_join_host).
+
+    The build side is copied in and built. The probe side streams through in chunks of
+    ``chunk_rows`` rows, with uploads, probes and downloads overlapped. Keys are a tensor (with
+    ``*_validity``) or a list of tensors / (tensor, validity) pairs. Payloads carry no NULLs.
+    ``capacity`` defaults to the probe row count, and ``out`` to pinned host buffers of that size.
+    More matches than ``capacity`` raise SJ_ERR_CAPACITY, which reports the count."""
+    def keys_of(k, v):
+        if isinstance(k, (list, tuple)):
+            if v is not None:
+                raise ValueError("pass (tensor, validity) pairs for composite keys")
+            pairs = [_as_pair(x) for x in k]
+        else:
+            pairs = [(k, v)]
+        return _cols([_host_column(t, vv) for t, vv in pairs]), len(pairs), pairs[0][0]
+    bcols, nkeys, _ = keys_of(build_keys, build_validity)
+    pcols, pk_n, first = keys_of(probe_keys, probe_validity)
+    if pk_n != nkeys:
+        raise ValueError("build and probe have different numbers of key columns")
+    pp = [_as_pair(c)[0] for c in probe_payload]
+    bp = [_as_pair(c)[0] for c in build_payload]
+    if capacity is None:
+        capacity = out.probe_rid.numel() if out is not None else first.numel()
+    if out is None:
+        def host(n, dt):
+            return torch.empty(n, dtype=dt).pin_memory()
+        out = JoinOutput(0, host(capacity, torch.int32), host(capacity, torch.int32),
+                         [host(capacity, t.dtype) for t in pp], [host(capacity, t.dtype) for t in bp])
+    params = L.default_params(**{k: v for k, v in table_kwargs.items()})
+    cnt = ctypes.c_int64(0)
+    lib = L.load()
+    st = lib.sj_inner_join_host(
+        bcols, pcols, nkeys, _cols([_host_column(t) for t in pp]), len(pp), _cols([_host_column(t) for t in bp]),
+        len(bp), out.probe_rid.data_ptr() if out.probe_rid is not None else None,
+        out.build_rid.data_ptr() if out.build_rid is not None else None,
+        _cols([_mut(t, None) for t in out.probe_payload], L.SjMutColumn),
+        _cols([_mut(t, None) for t in out.build_payload], L.SjMutColumn), capacity, chunk_rows,
+        ctypes.byref(params), None, _stream_handle(stream), ctypes.byref(cnt))
+    L.check(st, "sj_inner_join_host")
+    out.count = cnt.value
+    if out.count > capacity:
+        raise L.SjError(L.SJ_ERR_CAPACITY, "sj_inner_join_host", f"{out.count} matches > capacity {capacity}")
+    return out
+
+
 def hash_partition(keys, columns, num_partitions: int, stream: Optional[torch.cuda.Stream] = None):
     """Reorder `columns` (tensors or (tensor, validity) pairs) by the hash partition of `keys` (a
     tensor, or a list of 1..4 key columns / pairs). Returns (partitioned columns, partitioned validity

@@ -105,6 +105,38 @@ def test_argument_validation_needs_no_gpu(built):
         _lib.check(_lib.SJ_ERR_INVALID, "x")
 
 
+def test_host_join_argument_validation_needs_no_gpu(built):
+    """sj_inner_join_host refuses payloads with NULLs, key-type mismatches and missing outputs before
+    any CUDA call."""
+    import numpy as np
+    from sirius_b200 import _lib
+    lib = _lib.load()
+    keys = np.arange(64, dtype=np.int64)
+    words = np.full(2, -1, dtype=np.int32)
+
+    def col(a, valid=None):
+        c = _lib.SjColumn()
+        c.data = a.ctypes.data
+        c.validity = valid.ctypes.data if valid is not None else None
+        c.num_rows = len(a)
+        c.type = _lib.SJ_INT64 if a.dtype == np.int64 else _lib.SJ_INT32
+        return c
+    cnt = ctypes.c_int64(-1)
+    pay = (_lib.SjColumn * 1)(col(keys, words))
+    out = (_lib.SjMutColumn * 1)()
+    st = lib.sj_inner_join_host(ctypes.byref(col(keys)), ctypes.byref(col(keys)), 1, pay, 1, None, 0, None, None,
+                                out, None, 0, 0, None, None, None, ctypes.byref(cnt))
+    assert st == _lib.SJ_ERR_INVALID and b"payload columns with NULLs" in lib.sj_last_error()
+    k32 = np.arange(64, dtype=np.int32)
+    st = lib.sj_inner_join_host(ctypes.byref(col(keys)), ctypes.byref(col(k32)), 1, None, 0, None, 0, None, None,
+                                None, None, 0, 0, None, None, None, ctypes.byref(cnt))
+    assert st == _lib.SJ_ERR_INVALID and b"key types differ" in lib.sj_last_error()
+    pay = (_lib.SjColumn * 1)(col(keys))
+    st = lib.sj_inner_join_host(ctypes.byref(col(keys)), ctypes.byref(col(keys)), 1, pay, 1, None, 0, None, None,
+                                None, None, 64, 0, None, None, None, ctypes.byref(cnt))
+    assert st == _lib.SJ_ERR_INVALID and b"output missing" in lib.sj_last_error()
+
+
 def test_library_missing_fails_loudly(tmp_path):
     from sirius_b200 import _lib
     with pytest.raises(FileNotFoundError):

@@ -418,110 +418,142 @@ __global__ void __launch_bounds__(kProbeThreads, 4) grouped_match_kernel(TableDe
 
 // ------------------------------------------------------------------------------------------------
 // GROUPED expand: output position j -> (entry e with m_off[e] <= j < m_off[e+1]) -> one row.
+//
+// Every warp works alone (no CTA barrier): it owns a contiguous range of 256-output tiles and, per
+// tile, stages the entries the tile touches (at most 257: every entry has at least one output) in
+// its own shared-memory area, finds each output's entry there, loads the build rows and stores.
+// Lane l handles outputs j0 + 32m + l (m < 8), so each store is one coalesced warp access. A
+// warp's first entry comes from a 32-ary search of m_off (5 steps for 32M entries); every later
+// tile starts at the entry the previous tile ended in.
 // ------------------------------------------------------------------------------------------------
 constexpr int kExpandThreads = 256;
+constexpr int kExpandWarps = kExpandThreads / 32;
 constexpr int kExpandItems = 8;
-constexpr int kExpandTile = kExpandThreads * kExpandItems;
+constexpr int kExpandOut = 32 * kExpandItems;  // outputs per warp tile
+constexpr int kExpandEnt = kExpandOut + 1;     // entries a tile can touch
 
-__device__ __forceinline__ int64_t upper_index(const int64_t* off, int64_t lo, int64_t hi, int64_t j) {
-  // largest e in [lo, hi] with off[e] <= j (off[lo] <= j assumed)
+// Largest e in [0, n) with off[e] <= j (off[0] <= j assumed), found by the whole warp: each step
+// compares 32 evenly spaced candidates and keeps the gap between the last one at or below j and
+// the next.
+__device__ __forceinline__ int64_t warp_upper_index(const int64_t* off, int64_t n, int64_t j) {
+  const int lane = threadIdx.x & 31;
+  int64_t lo = 0, hi = n - 1;  // off[lo] <= j; the answer is in [lo, hi]
   while (lo < hi) {
-    const int64_t mid = (lo + hi + 1) >> 1;
-    if (off[mid] <= j) lo = mid;
-    else hi = mid - 1;
+    const int64_t span = hi - lo;
+    const int64_t cand = lo + 1 + (span * lane) / 32;  // 32 candidates in (lo, hi]
+    const bool le = cand <= hi && __ldg(off + cand) <= j;
+    const unsigned m = __ballot_sync(kFullMask, le);
+    if (m == 0) {
+      hi = lo;  // every candidate (the first is lo + 1) is above j: the answer is lo
+    } else {
+      const int top = 31 - __clz(m);
+      const int64_t c_top = lo + 1 + (span * top) / 32;
+      const int64_t c_next = top < 31 ? lo + 1 + (span * (top + 1)) / 32 : hi + 1;
+      lo = c_top;
+      hi = c_next - 1;
+    }
   }
   return lo;
 }
 
-// Largest e in [e, hi] with off[e] <= j, starting from a known e with off[e] <= j: gallop forward
-// (1, 2, 4, ... entries) then bisect, so a thread whose next position is in the same or a nearby
-// group pays one or two comparisons instead of a full binary search.
-__device__ __forceinline__ int gallop_index(const int64_t* off, int e, int hi, int64_t j) {
-  int step = 1, lo = e;
-  while (lo + step <= hi && off[lo + step] <= j) {
-    lo += step;
-    step <<= 1;
-  }
-  const int top = lo + step <= hi ? lo + step - 1 : hi;
-  return (int)upper_index(off, lo, top, j);
-}
-
-// Thread t of a tile handles positions j0 + m*256 + t (m < 8: consecutive lanes write consecutive
-// positions). Entry lookups stay in shared memory; then every item's group-member load is issued,
-// then every item's record (or row id + payloads), then the stores — 8 independent load chains per
-// thread instead of one at a time.
-__global__ void __launch_bounds__(kExpandThreads) expand_kernel(const int32_t* __restrict__ m_row,
+// RS > 0: a compile-time output shape — row-store records of RS bytes holding the build row id and
+// one payload of RS / 2 bytes at offset RS / 2 (no validity), no probe payloads; one load per row.
+// RS = 0: the shape is read from `g` at run time.
+template <int RS>
+__global__ void __launch_bounds__(kExpandThreads, 4) expand_kernel(const int32_t* __restrict__ m_row,
                                                                 const int32_t* __restrict__ m_start,
                                                                 const int64_t* __restrict__ m_off,
                                                                 const unsigned long long* d_nent,
                                                                 const int32_t* __restrict__ grp_rid,
                                                                 GatherArgs g) {
-  __shared__ int64_t s_off[kExpandTile + 1];
-  __shared__ int32_t s_row[kExpandTile + 1];
-  __shared__ int32_t s_start[kExpandTile + 1];
-  __shared__ int64_t s_e0;
+  __shared__ int64_t s_off_all[kExpandWarps][kExpandEnt];
+  __shared__ int32_t s_row_all[kExpandWarps][kExpandEnt];
+  __shared__ int32_t s_start_all[kExpandWarps][kExpandEnt];
   const int lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
+  int64_t* s_off = s_off_all[warp];
+  int32_t* s_row = s_row_all[warp];
+  int32_t* s_start = s_start_all[warp];
   const int64_t nent = (int64_t)*d_nent;
   if (nent == 0) return;
-  const int64_t M = m_off[nent];
+  const int64_t M = __ldg(m_off + nent);
   const int64_t cap = M < g.capacity ? M : g.capacity;
-  const int64_t ntile = (cap + kExpandTile - 1) / kExpandTile;
-  const int64_t per_block = (ntile + gridDim.x - 1) / gridDim.x;
-  const int64_t t_lo = (int64_t)blockIdx.x * per_block;
-  const int64_t t_hi = t_lo + per_block < ntile ? t_lo + per_block : ntile;
+  const int64_t ntile = (cap + kExpandOut - 1) / kExpandOut;
+  const int64_t nwarps = (int64_t)gridDim.x * kExpandWarps;
+  const int64_t per_warp = (ntile + nwarps - 1) / nwarps;
+  const int64_t t_lo = ((int64_t)blockIdx.x * kExpandWarps + warp) * per_warp;
+  const int64_t t_hi = t_lo + per_warp < ntile ? t_lo + per_warp : ntile;
   if (t_lo >= t_hi) return;
-  if (threadIdx.x == 0) s_e0 = upper_index(m_off, 0, nent - 1, t_lo * kExpandTile);
-  __syncthreads();
-  int64_t e0 = s_e0;
+  int64_t e0 = warp_upper_index(m_off, nent, t_lo * kExpandOut);
   for (int64_t tile = t_lo; tile < t_hi; ++tile) {
-    const int64_t j0 = tile * kExpandTile;
-    const int64_t j1 = j0 + kExpandTile < cap ? j0 + kExpandTile : cap;
-    const int ne = (int)((nent - e0) < (kExpandTile + 1) ? (nent - e0) : (kExpandTile + 1));
-    for (int i = threadIdx.x; i < ne; i += kExpandThreads) {
-      s_off[i] = m_off[e0 + i];
-      s_row[i] = m_row[e0 + i];
-      s_start[i] = m_start[e0 + i];
+    const int64_t j0 = tile * kExpandOut;
+    const int64_t j1 = j0 + kExpandOut < cap ? j0 + kExpandOut : cap;
+    const int ne = (int)((nent - e0) < kExpandEnt ? (nent - e0) : kExpandEnt);
+    for (int i = lane; i < ne; i += 32) {
+      s_off[i] = __ldg(m_off + e0 + i);
+      s_row[i] = __ldg(m_row + e0 + i);
+      s_start[i] = __ldg(m_start + e0 + i);
     }
-    __syncthreads();
-    // 1. entries (shared memory only). Warp w covers positions j0 + m*256 + 32w + lane, 32
-    //    consecutive outputs per m. Lane m finds the entry of the warp's first position for item m
-    //    (binary search); the entries of the 32 lanes are then that entry plus the number of entry
-    //    starts at or below each lane: the next 31 starts are loaded one per lane and their lane
-    //    offsets OR-ed into a mask, so a lane's entry is one popc away.
+    __syncwarp();
+    // 1. entries (shared memory only): eb = the entry of the warp's first position of item m; the
+    //    next 31 entry starts are read one per lane and OR-ed into a mask of lane offsets, so a
+    //    lane's entry is eb plus the starts at or below it
     int32_t row[kExpandItems], gi[kExpandItems];
-    {
-      const int warp = threadIdx.x >> 5;
-      const int64_t jw0 = j0 + 32 * warp;  // warp's first position for m = 0
-      int eb = 0;
-      if (lane < kExpandItems) {
-        const int64_t jb = jw0 + (int64_t)lane * kExpandThreads;
-        eb = jb < j1 ? (int)upper_index(s_off, 0, ne - 1, jb) : 0;
-      }
+    int eb = 0;
 #pragma unroll
-      for (int m = 0; m < kExpandItems; ++m) {
-        const int64_t jb = jw0 + (int64_t)m * kExpandThreads;
-        const int e_base = __shfl_sync(kFullMask, eb, m);
-        const int64_t j = jb + lane;
-        row[m] = 0;
-        gi[m] = -1;
-        if (jb >= j1) continue;  // warp-uniform
-        const int nb = e_base + 1 + lane;
-        const int64_t rel = (lane < 31 && nb < ne) ? s_off[nb] - jb : 64;
-        const unsigned starts = __reduce_or_sync(kFullMask, rel < 32 ? (1u << rel) : 0u);
-        const unsigned upto = lane == 31 ? kFullMask : ((2u << lane) - 1u);
-        const int e = e_base + __popc(starts & upto);
-        if (j < j1) {
-          row[m] = s_row[e];
-          gi[m] = s_start[e] + (int32_t)(j - s_off[e]);
-        }
+    for (int m = 0; m < kExpandItems; ++m) {
+      const int64_t jb = j0 + 32 * m;
+      const int64_t j = jb + lane;
+      row[m] = 0;
+      gi[m] = -1;
+      if (jb >= j1) continue;  // warp-uniform
+      const int nb = eb + 1 + lane;
+      const int64_t rel = (lane < 31 && nb < ne) ? s_off[nb] - jb : 64;
+      const unsigned starts = __reduce_or_sync(kFullMask, rel < 32 ? (1u << rel) : 0u);
+      const unsigned upto = lane == 31 ? kFullMask : ((2u << lane) - 1u);
+      const int e = eb + __popc(starts & upto);
+      if (j < j1) {
+        row[m] = s_row[e];
+        gi[m] = s_start[e] + (int32_t)(j - s_off[e]);
       }
+      // the entry of position jb + 32: lane 31's entry, or the next one if it starts right there
+      const int e31 = __shfl_sync(kFullMask, e, 31);
+      eb = e31 + ((e31 + 1 < ne && s_off[e31 + 1] == jb + 32) ? 1 : 0);
     }
     // 2. group members (table positions)
     int32_t pos[kExpandItems];
 #pragma unroll
     for (int m = 0; m < kExpandItems; ++m) pos[m] = gi[m] < 0 ? 0 : grp_rid ? __ldg(grp_rid + gi[m]) : gi[m];
     // 3. build side: one row-store record per item, or row id (+ payloads by row id / position)
-    if (g.rec) {
+    if constexpr (RS == 8 || RS == 16) {
+      uint32_t rid[kExpandItems];
+      uint64_t fv[kExpandItems];
+#pragma unroll
+      for (int m = 0; m < kExpandItems; ++m) {
+        rid[m] = 0;
+        fv[m] = 0;
+        if (gi[m] < 0) continue;
+        const char* rp = static_cast<const char*>(g.rec) + (int64_t)pos[m] * RS;
+        if constexpr (RS == 8) {
+          const uint2 x = __ldg(reinterpret_cast<const uint2*>(rp));
+          rid[m] = x.x;
+          fv[m] = x.y;
+        } else {
+          const uint4 x = __ldg(reinterpret_cast<const uint4*>(rp));
+          rid[m] = x.x;
+          fv[m] = ((uint64_t)x.w << 32) | x.z;
+        }
+      }
+#pragma unroll
+      for (int m = 0; m < kExpandItems; ++m) {
+        if (gi[m] < 0) continue;
+        const int64_t j = j0 + 32 * m + lane;
+        if (g.out_prid) __stcs(g.out_prid + j, row[m]);
+        if (g.out_brid) __stcs(g.out_brid + j, (int32_t)rid[m]);
+        if constexpr (RS == 8) __stcs(static_cast<unsigned int*>(g.bout[0].data) + j, (unsigned int)fv[m]);
+        else __stcs(static_cast<unsigned long long*>(g.bout[0].data) + j, (unsigned long long)fv[m]);
+      }
+    } else if (g.rec) {
       constexpr int kHalf = kExpandItems / 2;  // 4 records (up to 32 registers) in flight at a time
 #pragma unroll
       for (int h = 0; h < 2; ++h) {
@@ -535,7 +567,7 @@ __global__ void __launch_bounds__(kExpandThreads) expand_kernel(const int32_t* _
 #pragma unroll
         for (int q = 0; q < kHalf; ++q) {
           const int m = h * kHalf + q;
-          const int64_t j = j0 + (int64_t)m * kExpandThreads + threadIdx.x;
+          const int64_t j = j0 + 32 * m + lane;
           const bool live = gi[m] >= 0;
           if (live && g.out_prid) __stcs(g.out_prid + j, row[m]);
           if (live && g.out_brid) __stcs(g.out_brid + j, (int32_t)r[q].w[0]);
@@ -555,7 +587,7 @@ __global__ void __launch_bounds__(kExpandThreads) expand_kernel(const int32_t* _
       for (int m = 0; m < kExpandItems; ++m) rid[m] = gi[m] >= 0 ? brid_of(g, pos[m]) : 0;
 #pragma unroll
       for (int m = 0; m < kExpandItems; ++m) {
-        const int64_t j = j0 + (int64_t)m * kExpandThreads + threadIdx.x;
+        const int64_t j = j0 + 32 * m + lane;
         const bool live = gi[m] >= 0;
         if (live && g.out_prid) __stcs(g.out_prid + j, row[m]);
         if (live && g.out_brid) __stcs(g.out_brid + j, rid[m]);
@@ -575,14 +607,14 @@ __global__ void __launch_bounds__(kExpandThreads) expand_kernel(const int32_t* _
       }
     }
     // 4. probe payloads (by probe row)
-    for (int c = 0; c < g.n_pin; ++c) {
+    for (int c = 0; c < (RS > 0 ? 0 : g.n_pin); ++c) {
       const PayloadIn in = g.pin[c];
       uint64_t v[kExpandItems];
 #pragma unroll
       for (int m = 0; m < kExpandItems; ++m) v[m] = gi[m] >= 0 ? pl_load(in, row[m]) : 0;
 #pragma unroll
       for (int m = 0; m < kExpandItems; ++m) {
-        const int64_t j = j0 + (int64_t)m * kExpandThreads + threadIdx.x;
+        const int64_t j = j0 + 32 * m + lane;
         const bool live = gi[m] >= 0;
         if (live) store_elem_cs(g.pout[c].data, j, in.width, v[m]);
         if (has_validity(in)) {
@@ -591,10 +623,8 @@ __global__ void __launch_bounds__(kExpandThreads) expand_kernel(const int32_t* _
         }
       }
     }
-    __syncthreads();
-    if (threadIdx.x == 0) s_e0 = e0 + upper_index(s_off, 0, ne - 1, j1);
-    __syncthreads();
-    e0 = s_e0;
+    e0 += eb;      // the entry of position j0 + 256: where the next tile starts
+    __syncwarp();  // every lane is done with this tile's staged entries
   }
 }
 
@@ -882,9 +912,19 @@ sj_status probe_gather(const sj_table* t, const sj_column& p, const GatherSpec& 
     KernelTimer timer("scan", s);
     device_exclusive_scan<int32_t, int64_t>(m_cnt, m_off, d_nent, 0, tmp, s);
   }
-  const int grid = sm_count(t->device) * 4;
+  // every block resident at once: a warp's tile range is fixed, so a second wave would be a tail
+  // the compile-time shape: records [row id | one 4- or 8-byte payload], nothing else gathered
+  int rs = 0;
+  if (g.rec && g.n_pin == 0 && g.n_bin == 1 && g.rec_voff[0] < 0 && !g.bout[0].valid &&
+      (g.rec_stride == 8 || g.rec_stride == 16) && g.bin[0].width * 2 == g.rec_stride &&
+      g.rec_off[0] * 2 == g.rec_stride)
+    rs = g.rec_stride;
+  auto kernel = rs == 8 ? expand_kernel<8> : rs == 16 ? expand_kernel<16> : expand_kernel<0>;
+  int per_sm = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kExpandThreads, 0);
+  const int grid = sm_count(t->device) * std::max(1, per_sm);
   KernelTimer timer("expand", s);
-  expand_kernel<<<grid, kExpandThreads, 0, s>>>(m_row, m_start, m_off, d_nent, t->grp_rid, g);
+  kernel<<<grid, kExpandThreads, 0, s>>>(m_row, m_start, m_off, d_nent, t->grp_rid, g);
   SJ_CUDA_TRY(cudaGetLastError());
   return SJ_OK;
 }

@@ -342,3 +342,23 @@ def test_output_aggregation_modes(cuda, agg, pbits):
     for attach in (False, True):
         got, info = gpu_join(inp, cuda, attach=attach, aggregation=agg, partition_bits=pbits)
         assert_same_rows(got, oracle_join(inp))
+
+
+@pytest.mark.parametrize("pdt", [np.int32, np.int64])
+@pytest.mark.parametrize("pbits", [-1, 3])
+@pytest.mark.parametrize("probe_nulls", [False, True])
+def test_grouped_single_attached_payload_shapes(cuda, pdt, pbits, probe_nulls):
+    """A GROUPED table with one attached 4- or 8-byte payload and no probe payload: the expand's
+    compile-time record shapes (8- and 16-byte records). Skewed groups span many output tiles."""
+    rng = np.random.default_rng(31)
+    nb, npr = 200_000, 600_001
+    bk = np.concatenate([rng.integers(0, 40_000, nb - 3000), np.full(3000, 7)]).astype(np.int64)
+    rng.shuffle(bk)
+    pk = rng.integers(-1000, 41_000, npr).astype(np.int64)
+    pk[rng.random(npr) < 0.001] = 7  # a key with 3,000+ copies: one probe row spans several tiles
+    bp = [rng.integers(-2**31, 2**31 - 1, nb).astype(pdt)]
+    pv = O.pack_validity(rng.random(npr) > 0.1) if probe_nulls else None
+    inp = D.JoinInput("grouped-shapes", bk, pk, bp, [], None, pv)
+    got, info = gpu_join(inp, cuda, attach=True, partition_bits=pbits)
+    assert info.layout == 2
+    assert_same_rows(got, oracle_join(inp))

@@ -199,6 +199,22 @@ struct SlotOps<false> {
     pos = (int32_t)(sel & ((1u << rbits) - 1u));
     return any;
   }
+  // GROUPED tables (one slot per distinct key): the bucket as a whole, returning the slot index.
+  __device__ __forceinline__ static bool match_slot(const Bucket& bk, uint64_t ks, uint64_t kmask, int& slot) {
+    const uint32_t khi = (uint32_t)(ks >> 32), klo = (uint32_t)ks;
+    const uint32_t mhi = (uint32_t)(kmask >> 32), mlo = (uint32_t)kmask;
+    bool any = false;
+    int sel = 0;
+#pragma unroll
+    for (int q = 0; q < kSlots; ++q) {
+      const uint32_t hi = (uint32_t)(bk.a[q] >> 32), lo = (uint32_t)bk.a[q];
+      const bool m = ((hi & mhi) == khi) & ((lo & mlo) == klo);
+      sel = m ? q : sel;
+      any |= m;
+    }
+    slot = sel;
+    return any;
+  }
   __device__ __forceinline__ static bool open(const Bucket& bk) { return bk.a[kSlots - 1] == kEmpty; }
 };
 
@@ -221,6 +237,12 @@ struct SlotOps<true> {
     const bool m0 = bk.a[1] != kEmpty && bk.a[0] == kb;
     const bool m1 = bk.a[3] != kEmpty && bk.a[2] == kb;
     pos = (int32_t)(m0 ? bk.a[1] : bk.a[3]);
+    return m0 | m1;
+  }
+  __device__ __forceinline__ static bool match_slot(const Bucket& bk, uint64_t kb, uint64_t, int& slot) {
+    const bool m0 = bk.a[1] != kEmpty && bk.a[0] == kb;
+    const bool m1 = bk.a[3] != kEmpty && bk.a[2] == kb;
+    slot = m0 ? 0 : 1;
     return m0 | m1;
   }
   __device__ __forceinline__ static bool open(const Bucket& bk) { return bk.a[3] == kEmpty; }

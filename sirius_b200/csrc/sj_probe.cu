@@ -317,8 +317,14 @@ __global__ void __launch_bounds__(kProbeThreads, 4) probe_distinct_kernel(TableD
 
 // ------------------------------------------------------------------------------------------------
 // GROUPED pass A: find each probe row's group; compact (row, start, size); sum the output size.
+// A warp owns 32 * kMatchR consecutive probe rows per tile, lane l rows base + 32 j + l, so every
+// key load is one coalesced warp access; a bucket is tested as a whole (one slot per distinct
+// key); the rows with matches of row group j are ranked with one ballot and written at
+// base + (earlier groups) + popc(ballot_j & lanes below), one atomicAdd per warp tile.
 // ------------------------------------------------------------------------------------------------
-template <typename K, bool WIDE, bool VEC, bool COMPACT>
+constexpr int kMatchR = 4;
+
+template <typename K, bool WIDE, bool COMPACT>
 __global__ void __launch_bounds__(kProbeThreads, 4) grouped_match_kernel(TableDev t, const K* __restrict__ keys,
                                                                           const uint32_t* __restrict__ kv,
                                                                           int64_t kvoff, int64_t n, int32_t* m_row,
@@ -326,55 +332,62 @@ __global__ void __launch_bounds__(kProbeThreads, 4) grouped_match_kernel(TableDe
                                                                           unsigned long long* d_nent,
                                                                           unsigned long long* d_total) {
   using Ops = SlotOps<WIDE>;
-  __shared__ int32_t s_e[kWarpsPerCta][3][kStage];
+  constexpr int R = kMatchR;
   const int lane = threadIdx.x & 31;
-  const int warp = threadIdx.x >> 5;
-  const int64_t per_cta = (int64_t)blockDim.x * KPT;
-  const int64_t tiles = (n + per_cta - 1) / per_cta;
+  const unsigned below = (1u << lane) - 1u;
+  const int64_t wtiles = (n + 32 * R - 1) / (32 * R);
+  const int64_t wstride = (int64_t)gridDim.x * (blockDim.x >> 5);
+  const uint64_t kmask = ~((1ull << t.rbits) - 1);
   unsigned long long total = 0;
-  for (int64_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
-    const int64_t row0 = tile * per_cta + (int64_t)threadIdx.x * KPT;
-    K k[KPT];
-    load_keys<K>(keys, row0, n, VEC, k);
-    uint32_t act = live_rows<K>(t, k, row0, n, kv, kvoff);
-    int32_t slot[KPT];
-    uint32_t b[KPT];
-    uint64_t ks[KPT];
-    const uint64_t kmask = ~((1ull << t.rbits) - 1);
+  for (int64_t wt = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); wt < wtiles; wt += wstride) {
+    const int64_t r0 = wt * 32 * R + lane;
+    K k[R];
+    uint32_t act = 0;
+    int32_t slot[R];
 #pragma unroll
-    for (int j = 0; j < KPT; ++j) {
+    for (int j = 0; j < R; ++j) {
+      const int64_t r = r0 + 32 * j;
+      k[j] = r < n ? __ldcs(keys + r) : (K)0;
       slot[j] = -1;
+    }
+#pragma unroll
+    for (int j = 0; j < R; ++j) {
+      const int64_t r = r0 + 32 * j;
+      if (r >= n) continue;
+      if (!bit_valid(kv, kvoff, r)) {
+        if (t.null_group >= 0) slot[j] = t.null_group;  // NULLs equal: the NULL group
+      } else if (in_range(t, k[j])) {
+        act |= 1u << j;
+      }
+    }
+    uint32_t b[R];
+    uint64_t ks[R];
+#pragma unroll
+    for (int j = 0; j < R; ++j) {
       const uint64_t kb = key_u64<K>(k[j]);
       b[j] = home_bucket(t, kb);
       ks[j] = Ops::probe_key((uint64_t)(long long)k[j] - (uint64_t)t.kmin, kb, t.rbits);
-      if (t.null_group >= 0 && row0 + j < n && !bit_valid(kv, kvoff, row0 + j)) slot[j] = t.null_group;
     }
     for (uint32_t step = 0; act && step <= t.segmask; ++step) {
-      Bucket bk[KPT];
+      Bucket bk[R];
 #pragma unroll
-      for (int j = 0; j < KPT; ++j)
+      for (int j = 0; j < R; ++j)
         if (act >> j & 1u) bk[j] = load_bucket<true>(t.slots, b[j]);
 #pragma unroll
-      for (int j = 0; j < KPT; ++j) {
+      for (int j = 0; j < R; ++j) {
         if (!(act >> j & 1u)) continue;
-        bool done = false;
-#pragma unroll
-        for (int q = 0; q < Ops::kSlots; ++q) {
-          if (!done && Ops::match_s(bk[j], q, ks[j], kmask)) {
-            slot[j] = (int32_t)(b[j] * Ops::kSlots + q);
-            done = true;
-          }
-          done |= Ops::empty(bk[j], q);
-        }
-        if (done) act &= ~(1u << j);
+        int q;
+        const bool m = Ops::match_slot(bk[j], ks[j], kmask, q);
+        if (m) slot[j] = (int32_t)(b[j] * Ops::kSlots + q);
+        if (m || Ops::open(bk[j])) act &= ~(1u << j);
         else b[j] = next_bucket(b[j], t.segmask);
       }
     }
-    int32_t start[KPT], cnt[KPT];
+    int32_t start[R], cnt[R];
     uint32_t hit = 0;
 #pragma unroll
-    for (int j = 0; j < KPT; ++j) {
-      cnt[j] = 0;
+    for (int j = 0; j < R; ++j) {
+      start[j] = cnt[j] = 0;
       if (slot[j] >= 0) {
         start[j] = __ldg(t.grp_off + slot[j]);
         cnt[j] = __ldg(t.grp_off + slot[j] + 1) - start[j];
@@ -383,31 +396,27 @@ __global__ void __launch_bounds__(kProbeThreads, 4) grouped_match_kernel(TableDe
       }
     }
     if (COMPACT) {
-      // stage (row, start, size) in compacted order, then write the warp's range coalesced
-      const uint32_t c = __popc(hit);
-      const uint32_t incl = warp_inclusive_sum(c);
-      const uint32_t tot = __shfl_sync(kFullMask, incl, 31);
+      unsigned bal[R];
+      uint32_t tot = 0;
+#pragma unroll
+      for (int j = 0; j < R; ++j) {
+        bal[j] = __ballot_sync(kFullMask, (hit >> j) & 1u);
+        tot += __popc(bal[j]);
+      }
       if (tot) {
         unsigned long long base = 0;
         if (lane == 0) base = atomicAdd(d_nent, (unsigned long long)tot);
         base = __shfl_sync(kFullMask, base, 0);
-        uint32_t sp = incl - c;
 #pragma unroll
-        for (int j = 0; j < KPT; ++j) {
+        for (int j = 0; j < R; ++j) {
           if (hit >> j & 1u) {
-            s_e[warp][0][sp] = (int32_t)(row0 + j);
-            s_e[warp][1][sp] = start[j];
-            s_e[warp][2][sp] = cnt[j];
-            ++sp;
+            const unsigned long long p = base + __popc(bal[j] & below);
+            m_row[p] = (int32_t)(r0 + 32 * j);
+            m_start[p] = start[j];
+            m_cnt[p] = cnt[j];
           }
+          base += __popc(bal[j]);
         }
-        __syncwarp();
-        for (uint32_t i = lane; i < tot; i += 32) {
-          m_row[base + i] = s_e[warp][0][i];
-          m_start[base + i] = s_e[warp][1][i];
-          m_cnt[base + i] = s_e[warp][2][i];
-        }
-        __syncwarp();
       }
     }
   }
@@ -673,12 +682,15 @@ static void dispatch_distinct(const sj_table* t, const sj_column& p, const int64
 #undef SJ_D
 }
 
-template <typename K, bool WIDE, bool VEC, bool COMPACT>
+template <typename K, bool WIDE, bool COMPACT>
 static void launch_match(const sj_table* t, const sj_column& p, int32_t* m_row, int32_t* m_start, int32_t* m_cnt,
                          unsigned long long* d_nent, unsigned long long* d_total, cudaStream_t s) {
   const int block = kProbeThreads;
   KernelTimer timer(COMPACT ? "grouped_match" : "grouped_count", s);
-  grouped_match_kernel<K, WIDE, VEC, COMPACT><<<probe_grid(t, p.num_rows, block), block, 0, s>>>(
+  const int64_t wtiles = (p.num_rows + 32 * kMatchR - 1) / (32 * kMatchR);
+  const int64_t cap = (int64_t)sm_count(t->device) * std::max(1, t->params.ctas_per_sm);
+  const int grid = (int)std::max<int64_t>(1, std::min(cap, (wtiles + kWarpsPerCta - 1) / kWarpsPerCta));
+  grouped_match_kernel<K, WIDE, COMPACT><<<grid, block, 0, s>>>(
       table_dev(t), static_cast<const K*>(p.data), p.validity, p.validity_offset, p.num_rows, m_row, m_start,
       m_cnt, d_nent, d_total);
 }
@@ -687,14 +699,13 @@ template <bool COMPACT>
 static void dispatch_match(const sj_table* t, const sj_column& p, int32_t* m_row, int32_t* m_start, int32_t* m_cnt,
                            unsigned long long* d_nent, unsigned long long* d_total, cudaStream_t s) {
   const bool wide = t->slot_kind == SJ_SLOT_WIDE128;
-  const bool vec = aligned16(p.data);
-#define SJ_M(K, W, V) launch_match<K, W, V, COMPACT>(t, p, m_row, m_start, m_cnt, d_nent, d_total, s)
+#define SJ_M(K, W) launch_match<K, W, COMPACT>(t, p, m_row, m_start, m_cnt, d_nent, d_total, s)
   if (t->key_type == SJ_INT32) {
-    if (wide) { if (vec) SJ_M(int32_t, true, true); else SJ_M(int32_t, true, false); }
-    else { if (vec) SJ_M(int32_t, false, true); else SJ_M(int32_t, false, false); }
+    if (wide) SJ_M(int32_t, true);
+    else SJ_M(int32_t, false);
   } else {
-    if (wide) { if (vec) SJ_M(int64_t, true, true); else SJ_M(int64_t, true, false); }
-    else { if (vec) SJ_M(int64_t, false, true); else SJ_M(int64_t, false, false); }
+    if (wide) SJ_M(int64_t, true);
+    else SJ_M(int64_t, false);
   }
 #undef SJ_M
 }

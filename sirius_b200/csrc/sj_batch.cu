@@ -224,6 +224,104 @@ __device__ void probe_tile(const BatchDev& P, const BJoin& J, int32_t join, int3
   }
 }
 
+// Group width 1: each lane keeps kBatchR probe rows in flight (rows base + 32 j + lane, so every
+// key load is one coalesced warp access). Two rows per lane (80 registers, 3 CTAs of 256 per SM)
+// beat one row (4 CTAs) by 18 % and four rows (105 registers, 2 CTAs) by 36 % on 4,096 joins. A step probes one bucket for each of the lane's live
+// rows; the matches of all its rows are reserved with one atomicAdd per warp and step. When every
+// row has at most one match in the step (unique build keys), group j's hit lanes are ranked with a
+// ballot so each output column is written as one contiguous run per group; otherwise positions
+// follow (lane, row group, slot) order. A row stops at its first bucket with an EMPTY slot (its
+// matches there still count) or once the whole table has been scanned.
+constexpr int kBatchR = 2;
+
+template <typename K>
+__device__ void probe_tile_r(const BatchDev& P, const BJoin& J, int32_t join, int32_t tile) {
+  constexpr int S = BTable<K>::kSlots;
+  constexpr int R = kBatchR;
+  const int lane = threadIdx.x & 31;
+  const int nwarps = blockDim.x >> 5;
+  const int64_t lo = (int64_t)tile * P.tile_rows;
+  const int64_t hi = min(J.np, lo + P.tile_rows);
+  const uint64_t mask = (1ull << J.log2_nb) - 1;
+  for (int64_t base = lo + (int64_t)(threadIdx.x >> 5) * 32 * R; base < hi; base += (int64_t)nwarps * 32 * R) {
+    K k[R];
+    uint64_t b[R];
+    uint32_t act = 0;
+#pragma unroll
+    for (int j = 0; j < R; ++j) {
+      const int64_t i = base + 32 * j + lane;
+      const bool live = i < hi && bit_valid(J.pvalid, J.pvoff, i);
+      k[j] = live ? load_key<K>(J.pkey, i) : (K)0;
+      b[j] = live ? bhome<K>(J, k[j]) : 0;
+      if (live) act |= 1u << j;
+    }
+    for (uint64_t step = 0; __any_sync(kFullMask, act != 0); ++step) {
+      uint32_t m[R];
+      int32_t rid[R][4];
+      uint32_t cnt = 0;
+#pragma unroll
+      for (int j = 0; j < R; ++j) {
+        m[j] = 0;
+        if (!(act >> j & 1u)) continue;
+        bool has_empty = false;
+        m[j] = BTable<K>::probe(P.arena, J.bucket_off + b[j], k[j], has_empty, rid[j]);
+        cnt += __popc(m[j]);
+        if (has_empty || step >= mask) act &= ~(1u << j);
+        else b[j] = (b[j] + 1) & mask;
+      }
+      // write one match: output position p, probe row i, build row id rid
+      auto put = [&](int64_t p, int64_t i, int32_t brow) {
+        if (p >= J.capacity) return;
+        if (J.out_prid) J.out_prid[p] = (int32_t)i;
+        if (J.out_brid) J.out_brid[p] = brow;
+        if (J.ppay.data) {
+          store_elem(J.out_ppay.data, p, J.ppay.width, load_elem(J.ppay.data, i, J.ppay.width));
+          if (J.ppay.valid && bit_valid(J.ppay.valid, J.ppay.voff, i)) set_out_bit(J.out_ppay.valid, p);
+        }
+        if (J.bpay.data) {
+          store_elem(J.out_bpay.data, p, J.bpay.width, load_elem(J.bpay.data, brow, J.bpay.width));
+          if (J.bpay.valid && bit_valid(J.bpay.valid, J.bpay.voff, brow)) set_out_bit(J.out_bpay.valid, p);
+        }
+      };
+      bool single = true;  // at most one match per row in this step (always so for unique builds)
+#pragma unroll
+      for (int j = 0; j < R; ++j) single &= (m[j] & (m[j] - 1u)) == 0;
+      if (__all_sync(kFullMask, single)) {
+        // row-group-major positions: group j's hit lanes write one contiguous run per column
+        unsigned bal[R];
+        uint32_t tot = 0;
+#pragma unroll
+        for (int j = 0; j < R; ++j) {
+          bal[j] = __ballot_sync(kFullMask, m[j] != 0);
+          tot += __popc(bal[j]);
+        }
+        if (tot == 0) continue;
+        unsigned long long pos = 0;
+        if (lane == 0) pos = atomicAdd(P.counts + join, (unsigned long long)tot);
+        pos = __shfl_sync(kFullMask, pos, 0);
+        const unsigned below = (1u << lane) - 1u;
+#pragma unroll
+        for (int j = 0; j < R; ++j) {
+          int32_t brow = 0;
+#pragma unroll
+          for (int q = 0; q < S; ++q) brow = (m[j] >> q & 1u) ? rid[j][q] : brow;
+          if (m[j]) put((int64_t)(pos + __popc(bal[j] & below)), base + 32 * j + lane, brow);
+          pos += __popc(bal[j]);
+        }
+      } else {
+        // duplicates in one bucket: lane-major positions
+        const unsigned long long pos0 = warp_reserve(P.counts + join, cnt);
+        uint32_t r = 0;
+#pragma unroll
+        for (int j = 0; j < R; ++j)
+#pragma unroll
+          for (int q = 0; q < S; ++q)
+            if (m[j] >> q & 1u) put((int64_t)pos0 + r++, base + 32 * j + lane, rid[j][q]);
+      }
+    }
+  }
+}
+
 __device__ __forceinline__ void wait_built(const BatchDev& P, int32_t join, int32_t need) {
   if (threadIdx.x == 0) {
     unsigned spins = 0;
@@ -259,7 +357,8 @@ __global__ void batch_persistent_kernel(BatchDev P) {
       }
     } else {
       wait_built(P, item.join, J.build_tiles);
-      probe_tile<K, G>(P, J, item.join, item.tile);
+      if constexpr (G == 1) probe_tile_r<K>(P, J, item.join, item.tile);
+      else probe_tile<K, G>(P, J, item.join, item.tile);
     }
   }
 }
@@ -273,7 +372,10 @@ __global__ void batch_build_one_kernel(BatchDev P, int32_t j) {
 template <typename K, int G>
 __global__ void batch_probe_one_kernel(BatchDev P, int32_t j, int32_t probe_tiles) {
   const BJoin J = P.joins[j];
-  for (int32_t t = blockIdx.x; t < probe_tiles; t += gridDim.x) probe_tile<K, G>(P, J, j, t);
+  for (int32_t t = blockIdx.x; t < probe_tiles; t += gridDim.x) {
+    if constexpr (G == 1) probe_tile_r<K>(P, J, j, t);
+    else probe_tile<K, G>(P, J, j, t);
+  }
 }
 
 }  // namespace sj

@@ -376,7 +376,7 @@ __global__ void __launch_bounds__(kPartThreads, 3) part_scatter_fast_kernel(Part
       const unsigned slot = toff[pr[j]] + rank[j];
       skey[slot] = kk[j];
       srid[slot] = (int32_t)(t0 + j * kPartThreads + tid);
-      sdst[slot] = LOCAL ? (uint32_t)t0 + slot : (uint32_t)cur[pr[j]] + rank[j];
+      if (!LOCAL) sdst[slot] = (uint32_t)cur[pr[j]] + rank[j];  // LOCAL: the tile's own rows
 #pragma unroll
       for (int c = 0; c < NP; ++c) reinterpret_cast<uint64_t*>(sm + m.pay[c])[slot] = pv[c][j];
     }
@@ -384,7 +384,7 @@ __global__ void __launch_bounds__(kPartThreads, 3) part_scatter_fast_kernel(Part
     // 4. loads of the next tile go out before this tile's write-out
     if (t0 + kTile < hi) fast_load_tile<K, NP>(s, t0 + kTile, hi, kk, pv, live);
     for (unsigned slot = tid; slot < tile_valid; slot += kPartThreads) {
-      const uint32_t pos = sdst[slot];
+      const uint32_t pos = LOCAL ? (uint32_t)t0 + slot : sdst[slot];
       okeys[pos] = skey[slot];
       d.rid[pos] = srid[slot];
 #pragma unroll

@@ -238,7 +238,14 @@ SJ_EXPORT sj_status sj_table_destroy(sj_table* table, sj_stream_t stream);
 
 SJ_EXPORT sj_status sj_table_get_info(const sj_table* table, sj_table_info* info);
 
-/* Count the INNER matches of the probe keys (the size pass cuDF runs before retrieval for the
+/* Probe keys of every sj_probe_* call: the table's number of key columns. A single key column
+ * may be of the other integer type than the table's (the reference's key casts,
+ * prepare_join_keys, src/op/sirius_physical_hash_join.cpp:1234-1291): INT32 probe keys widen
+ * exactly into an INT64 table; INT64 probe keys narrow exactly into an INT32 table when in range
+ * and otherwise never match (they stay non-NULL); a table whose INT32 keys span the whole INT32
+ * range refuses INT64 probes with SJ_ERR_INVALID. Composite-key columns may mix types freely.
+ *
+ * Count the INNER matches of the probe keys (the size pass cuDF runs before retrieval for the
  * multiset inner_join). Writes the count to *d_count (device int64). Stream-ordered. */
 SJ_EXPORT sj_status sj_probe_count(const sj_table* table, const sj_column* probe_keys,
                                    int32_t num_keys, const sj_alloc* alloc, sj_stream_t stream,

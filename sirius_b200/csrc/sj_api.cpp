@@ -220,6 +220,11 @@ static sj_status probe_keys_of(const sj_table* t, const sj_column* keys, int32_t
                                cudaStream_t s, Scratch& buf, sj_column* out) {
   if (t->kpack.n > 1) return pack_probe_keys(t->kpack, keys, num_keys, a, s, buf, out);
   if (num_keys != 1) return set_error(SJ_ERR_INVALID, "the table was built on one key column");
+  if ((keys[0].type == SJ_INT32 || keys[0].type == SJ_INT64) && keys[0].type != t->key_type &&
+      (t->key_type == SJ_INT32 || t->key_type == SJ_INT64)) {
+    SJ_TRY(validate_column(&keys[0], "probe key", true));
+    return cast_probe_keys(t->key_type, t->kmin, t->kmax, keys[0], a, s, buf, out);
+  }
   *out = keys[0];
   return SJ_OK;
 }

@@ -184,6 +184,10 @@ sj_status validate_column(const sj_column* c, const char* what, bool key);
 // Composite keys (sj_keys.cu): pack 2..4 key columns into one INT64 column held in `buf`.
 sj_status pack_build_keys(const sj_column* keys, int n_keys, bool nulls_equal, const Allocator& alloc,
                           cudaStream_t s, KeyPack* kp, Scratch& buf, sj_column* packed);
+// A single-column probe key of the other integer type, converted to the table's type `table_type`
+// (int32 -> int64 exactly; int64 -> int32 exactly in range, else a value outside [kmin, kmax]).
+sj_status cast_probe_keys(int32_t table_type, int64_t kmin, int64_t kmax, const sj_column& keys, const Allocator& alloc,
+                          cudaStream_t s, Scratch& buf, sj_column* out);
 sj_status pack_probe_keys(const KeyPack& kp, const sj_column* keys, int n_keys, const Allocator& alloc,
                           cudaStream_t s, Scratch& buf, sj_column* packed);
 

@@ -11,6 +11,7 @@
 // every build code. Keys whose ranges need more than 63 bits in total are refused.
 #include <algorithm>
 #include <climits>
+#include <limits>
 #include <string>
 
 #include "sj_device.cuh"
@@ -195,6 +196,52 @@ sj_status pack_probe_keys(const KeyPack& kp, const sj_column* keys, int n_keys, 
   int device = 0;
   cudaGetDevice(&device);
   return pack(key_cols(keys, n_keys), keys[0].num_rows, kp, any_null, alloc, s, buf, packed, device);
+}
+
+// ------------------------------------------------------------------------------------------------
+// Single-column probe keys of the other integer type than the table's (the reference casts key
+// columns to the join's comparison type, cudf::cast in prepare_join_keys,
+// src/op/sirius_physical_hash_join.cpp:1272-1284). int32 into an int64 table widens exactly;
+// int64 into an int32 table narrows values in the int32 range exactly and maps the others to
+// `miss`, an int32 value outside the table's key range, so they never match (they stay non-NULL:
+// LEFT, ANTI and MARK treat them as rows without a match). Validity passes through unchanged.
+// ------------------------------------------------------------------------------------------------
+template <typename In, typename Out>
+__global__ void __launch_bounds__(256) key_cast_kernel(const In* __restrict__ in, int64_t n, Out* out, long long miss) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const long long v = (long long)__ldg(in + i);
+    const bool fits = v >= (long long)std::numeric_limits<Out>::min() && v <= (long long)std::numeric_limits<Out>::max();
+    out[i] = (Out)(fits ? v : miss);
+  }
+}
+
+sj_status cast_probe_keys(int32_t table_type, int64_t kmin, int64_t kmax, const sj_column& keys, const Allocator& alloc,
+                          cudaStream_t s, Scratch& buf, sj_column* out) {
+  const int64_t n = keys.num_rows;
+  long long miss = 0;
+  if (table_type == SJ_INT32) {  // a value the table cannot hold
+    if (kmax < kmin) miss = 0;  // no valid build key: nothing matches anyway
+    else if (kmax < INT32_MAX) miss = kmax + 1;
+    else if (kmin > INT32_MIN) miss = kmin - 1;
+    else return set_error(SJ_ERR_INVALID, "int64 probe keys into an int32 table whose keys span the whole int32 range");
+  }
+  const size_t w = table_type == SJ_INT32 ? 4 : 8;
+  SJ_TRY(buf.get(alloc, (size_t)std::max<int64_t>(n, 1) * w, s));
+  *out = keys;
+  out->data = buf.ptr;
+  out->type = table_type;
+  if (n == 0) return SJ_OK;
+  int device = 0;
+  cudaGetDevice(&device);
+  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, (int64_t)sm_count(device) * 8));
+  if (table_type == SJ_INT64)
+    key_cast_kernel<int32_t, long long><<<grid, 256, 0, s>>>(static_cast<const int32_t*>(keys.data), n,
+                                                             buf.as<long long>(), 0);
+  else
+    key_cast_kernel<long long, int32_t><<<grid, 256, 0, s>>>(static_cast<const long long*>(keys.data), n,
+                                                             buf.as<int32_t>(), miss);
+  SJ_CUDA_TRY(cudaGetLastError());
+  return SJ_OK;
 }
 
 }  // namespace sj

@@ -69,3 +69,14 @@ def test_composite_keys_and_cross_table_consistency(cuda):
     for x, y, p in zip(b[0].tolist(), b[1].tolist(), pb.tolist()):
         if (x, y) in ta:
             assert ta[(x, y)] == p
+
+
+def test_int32_and_int64_keys_of_equal_value_share_partitions(cuda):
+    """The reference casts partition keys of mixed-type joins so both sides hash alike
+    (gpu_partition_impl.cpp:45-60); here the partition function sign-extends keys to 64 bits, so
+    equal values land in the same partition whatever their integer type."""
+    rng = np.random.default_rng(12)
+    v = rng.integers(-2**31, 2**31 - 1, 100_000)
+    a = _check(cuda, [v.astype(np.int32)], [None], [], [], 64)
+    b = _check(cuda, [v.astype(np.int64)], [None], [], [], 64)
+    assert np.array_equal(a, b)

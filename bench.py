@@ -699,7 +699,9 @@ def run_other(args):
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
-        tb = J.HashTable(bk, attach=bp, partition_bits=args.partition_bits)
+        tb = J.HashTable(bk, attach=bp, partition_bits=args.partition_bits, aggregation=args.aggregation,
+                         probe_kernel=args.probe_kernel, rows_per_lane=args.rows_per_lane,
+                         probe_partition_mb=args.probe_partition_mb, table_l2_priority=args.table_l2)
         e1.record()
         torch.cuda.synchronize()
         t_build.append(e0.elapsed_time(e1))

@@ -8,6 +8,7 @@
 //           full_join                                         -> sj_hash_table::full_join(...)
 //           semi_join + resolve_mark_join_result (:1461-1525) -> sj_hash_table::mark_join(...)
 //   gather  :1945-1954 gather_join_output(...)               -> (fused into the calls above)
+//   STANDARD RIGHT / RIGHT_SEMI / RIGHT_ANTI (:1879-1895)     -> right_join(...): sides swapped
 #include "sirius_hash_join_sj.hpp"
 
 #include <cuda_runtime_api.h>
@@ -23,11 +24,8 @@ namespace sirius::op::sj_adapter {
 
 namespace {
 
-// sj_alloc over an RMM resource: the join's device memory is the task's reservation.
-struct rmm_alloc_ctx {
-  rmm::device_async_resource_ref mr;
-};
-
+// sj_alloc over an RMM resource (ctx: an rmm_alloc_ctx): the join's device memory is the task's
+// reservation.
 void* rmm_alloc(void* ctx, size_t bytes, sj_stream_t s) {
   auto* c = static_cast<rmm_alloc_ctx*>(ctx);
   try {
@@ -117,7 +115,7 @@ void check(sj_status st, char const* where) {
 sj_hash_table::sj_hash_table(cudf::table_view const& build_keys, cudf::table_view const& build_payload,
                              cudf::null_equality nulls, bool unique_build_keys, rmm::cuda_stream_view stream,
                              rmm::device_async_resource_ref mr)
-  : mr_(mr), stream_(stream)
+  : alloc_ctx_{mr}, stream_(stream)
 {
   const std::vector<sj_column> keys = key_columns(build_keys);
   std::vector<sj_column> pay;
@@ -130,8 +128,9 @@ sj_hash_table::sj_hash_table(cudf::table_view const& build_keys, cudf::table_vie
   sj_default_params(&p);
   p.layout        = unique_build_keys ? SJ_LAYOUT_DISTINCT : SJ_LAYOUT_AUTO;
   p.null_equality = nulls == cudf::null_equality::EQUAL ? SJ_NULLS_EQUAL : SJ_NULLS_UNEQUAL;
-  rmm_alloc_ctx ctx{mr};
-  const sj_alloc a{&ctx, rmm_alloc, rmm_free};
+  // the table keeps this sj_alloc and frees through its context in sj_table_destroy: the context is
+  // the member alloc_ctx_, which lives as long as the table
+  const sj_alloc a{&alloc_ctx_, rmm_alloc, rmm_free};
   // sj_build_ex synchronizes the stream, as the operator does after building (:1622)
   check(sj_build_ex(keys.data(), (int32_t)keys.size(), pay.data(), (int32_t)pay.size(), &p, &a, raw(stream), &table_),
         "sj_build_ex");
@@ -272,6 +271,27 @@ std::unique_ptr<cudf::table> sj_hash_table::mark_join(cudf::table_view const& pr
   cols.push_back(std::make_unique<cudf::column>(cudf::data_type(cudf::type_id::BOOL8), n, std::move(mark),
                                                 std::move(mask), nc));
   return std::make_unique<cudf::table>(std::move(cols), stream);
+}
+
+std::unique_ptr<cudf::table> right_join(right_kind kind, cudf::table_view const& left_keys,
+                                        cudf::table_view const& left_cols, cudf::table_view const& right_keys,
+                                        cudf::table_view const& right_cols, cudf::null_equality nulls,
+                                        rmm::cuda_stream_view stream, rmm::device_async_resource_ref mr)
+{
+  const bool collect_left = kind == right_kind::RIGHT;
+  // build on the left side (its projected columns attached only when they are output)
+  const sj_hash_table table(left_keys, collect_left ? left_cols : cudf::table_view{}, nulls,
+                            /*unique_build_keys=*/false, stream, mr);
+  if (!collect_left)
+    return table.join(kind == right_kind::RIGHT_SEMI ? SJ_JOIN_SEMI : SJ_JOIN_ANTI, right_keys, right_cols, stream, mr);
+  // LEFT join of right over left gives [right columns..., left columns (NULL-padded)...]
+  auto swapped = table.join(SJ_JOIN_LEFT, right_keys, right_cols, stream, mr);
+  auto cols    = swapped->release();
+  std::vector<std::unique_ptr<cudf::column>> out;
+  const size_t n_right = static_cast<size_t>(right_cols.num_columns());
+  for (size_t c = n_right; c < cols.size(); ++c) out.push_back(std::move(cols[c]));
+  for (size_t c = 0; c < n_right; ++c) out.push_back(std::move(cols[c]));
+  return std::make_unique<cudf::table>(std::move(out), stream);
 }
 
 }  // namespace sirius::op::sj_adapter

@@ -34,6 +34,13 @@ std::vector<sj_column> key_columns(cudf::table_view const& keys);
 /// Throws rmm::out_of_memory for SJ_ERR_OOM, std::runtime_error otherwise (no-op for SJ_OK).
 void check(sj_status st, char const* where);
 
+/// The context of an sj_alloc over an RMM resource. libsj keeps the sj_alloc a table was built with
+/// and frees the table's memory through it in sj_table_destroy, so a context handed to sj_build_ex
+/// must live as long as the table: sj_hash_table holds it as a member.
+struct rmm_alloc_ctx {
+  rmm::device_async_resource_ref mr;
+};
+
 /// The built table of one BUILD_PROBE partition slot: replaces cudf::hash_join /
 /// cudf::distinct_hash_join in per_partition_build_state
 /// (src/include/op/sirius_physical_hash_join.hpp:409-421). It keeps a copy of the projected build
@@ -44,8 +51,11 @@ class sj_hash_table {
                 cudf::null_equality nulls, bool unique_build_keys, rmm::cuda_stream_view stream,
                 rmm::device_async_resource_ref mr);
   ~sj_hash_table();
+  // not copyable or movable: the built table refers to this object's allocator context
   sj_hash_table(sj_hash_table const&)            = delete;
   sj_hash_table& operator=(sj_hash_table const&) = delete;
+  sj_hash_table(sj_hash_table&&)                 = delete;
+  sj_hash_table& operator=(sj_hash_table&&)      = delete;
 
   /// INNER probe + gather_join_output in one call: returns the output table
   /// [probe_payload columns..., build payload columns...] (src/op/sirius_physical_hash_join.cpp:1350-1355).
@@ -76,11 +86,26 @@ class sj_hash_table {
                                    cudf::table_view const& probe_payload, cudf::table_view const* build_cols,
                                    rmm::cuda_stream_view stream, rmm::device_async_resource_ref mr) const;
 
+  rmm_alloc_ctx alloc_ctx_;  // the build's allocator context; the table frees through it
   sj_table* table_ = nullptr;
   std::vector<cudf::data_type> build_types_;
   std::vector<bool> build_nullable_;
-  rmm::device_async_resource_ref mr_;
   rmm::cuda_stream_view stream_;
 };
+
+/// The RIGHT family of STANDARD mode (src/op/sirius_physical_hash_join.cpp:1879-1895), run the way
+/// the reference runs it: with the sides swapped. The table is built on the LEFT keys (the left
+/// output columns attached for RIGHT) and probed with the RIGHT keys:
+///   RIGHT      = cudf::left_join(right_keys, left_keys)       -> [left columns (NULL where
+///                unmatched)..., right columns...]
+///   RIGHT_SEMI = filtered_join(left_keys).semi_join(right)    -> [right columns...]
+///   RIGHT_ANTI = filtered_join(left_keys).anti_join(right)    -> [right columns...]
+/// The column order is gather_join_output's (:1299-1359): left columns, then right columns, with
+/// the left side not collected for RIGHT_SEMI / RIGHT_ANTI.
+enum class right_kind { RIGHT, RIGHT_SEMI, RIGHT_ANTI };
+std::unique_ptr<cudf::table> right_join(right_kind kind, cudf::table_view const& left_keys,
+                                        cudf::table_view const& left_cols, cudf::table_view const& right_keys,
+                                        cudf::table_view const& right_cols, cudf::null_equality nulls,
+                                        rmm::cuda_stream_view stream, rmm::device_async_resource_ref mr);
 
 }  // namespace sirius::op::sj_adapter

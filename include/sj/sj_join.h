@@ -507,11 +507,16 @@ SJ_EXPORT sj_status sj_inner_join_host(const sj_column* build_keys, const sj_col
  * must not wait in the driver's allocator, and hosts whose allocator belongs to another component.
  * No counterpart in the reference: Sirius's join always allocates through its memory pool.
  * Every byte of scratch (hash table, build statistics, grouped-probe match list) comes from one
- * 64 MiB `static __device__` array per GPU, held by every GPU that loads this library until the
- * process exits; no cudaMalloc, cudaFree or allocator callback is used. Outputs follow
- * sj_probe_gather's contract (caller-provided device buffers, *d_count = matches). Inputs whose
- * worst-case scratch exceeds the arena are rejected with SJ_ERR_INVALID before any GPU work (about
- * 1M build rows with a few million probe rows fit). The table is never radix-partitioned.
+ * 64 MiB `static __device__` array per GPU; no cudaMalloc, cudaFree or allocator callback is used.
+ * The driver commits the array when it loads the library's device code: at the first call on a
+ * device under lazy module loading (CUDA_MODULE_LOADING=LAZY, the default since CUDA 12.2), at
+ * library load under EAGER. A caller whose memory will be fully committed later makes one warm-up
+ * call while 64 MiB are still free; every GPU that ran the entry point then holds the array until
+ * the process exits. Outputs follow sj_probe_gather's contract (caller-provided device buffers,
+ * *d_count = matches). Inputs whose worst-case scratch exceeds the array are rejected with
+ * SJ_ERR_INVALID before any GPU work; at load factor 0.5 that allows 2^19 build rows with up to
+ * 1.9M probe rows, or 2^20 build rows with up to 600K probe rows. The table is never
+ * radix-partitioned: every params field is honoured except partition_bits and probe_partition_mb.
  * All calls share the array and leave their data in it; each call re-initialises what it reads,
  * but calls that overlap on the GPU race: serialise them (one stream, or synchronise between).
  * The first call on a device looks up the array's device address (cudaGetSymbolAddress) with that
@@ -548,6 +553,15 @@ typedef struct sj_kernel_time {
 
 SJ_EXPORT void sj_timing_enable(int32_t on);
 SJ_EXPORT int32_t sj_timing_collect(sj_kernel_time* out, int32_t capacity);
+
+/* Test hook for the library's bounded device waits: runs, in one small kernel, the batched join's
+ * wait for a join's build tiles on a counter that nothing increments, and the TMA probe ring's wait
+ * for a stage's bulk copies on an mbarrier that nothing arrives on, each limited to `polls` polls
+ * (1..2^20). d_status: device int32[3]; after the stream, d_status[0] / d_status[1] are 1 when the
+ * build wait / the mbarrier wait gave up (as they must), 0 otherwise; d_status[2] is scratch. The
+ * library reports such a timeout as SJ_ERR_TIMEOUT (a batch's error word bit 0, a probe's negative
+ * count). No counterpart in the reference. Stream-ordered. */
+SJ_EXPORT sj_status sj_debug_wait_timeout(int32_t polls, sj_stream_t stream, int32_t* d_status);
 
 /* ABI version: major * 10000 + minor * 100 + patch. */
 SJ_EXPORT int32_t sj_version(void);

@@ -122,6 +122,7 @@ SIGNATURES = {
     "sj_status_string": (c_char_p, [c_int32]),
     "sj_last_error": (c_char_p, []),
     "sj_version": (c_int32, []),
+    "sj_debug_wait_timeout": (c_int32, [c_int32, c_void_p, c_void_p]),
     "sj_timing_enable": (None, [c_int32]),
     "sj_batch_plan_create": (c_int32, [_P(SjBatchJoin), c_int32, _P(SjBatchParams), _P(SjAlloc), c_void_p,
                                        _P(c_void_p)]),

@@ -324,14 +324,7 @@ __device__ void probe_tile_r(const BatchDev& P, const BJoin& J, int32_t join, in
 
 __device__ __forceinline__ void wait_built(const BatchDev& P, int32_t join, int32_t need) {
   if (threadIdx.x == 0) {
-    unsigned spins = 0;
-    while (*(volatile unsigned int*)(P.built + join) < (unsigned)need) {
-      if (++spins > kWaitLimit) {
-        atomicOr(P.error, 1);
-        break;
-      }
-      __nanosleep(128);
-    }
+    if (!wait_counter_at_least(P.built + join, (unsigned)need, kWaitLimit)) atomicOr(P.error, 1);
     __threadfence();
   }
   __syncthreads();

@@ -269,6 +269,19 @@ __device__ __forceinline__ bool bit_valid(const uint32_t* v, int64_t off, int64_
   return (__ldg(v + (b >> 5)) >> (b & 31)) & 1u;
 }
 
+// ---- bounded waits -----------------------------------------------------------------------------
+// Polls `*counter` (written by other CTAs) until it reaches `need`, sleeping ~128 ns between polls;
+// gives up after `polls` polls and returns false. One thread calls it; the caller publishes the
+// outcome to its CTA.
+__device__ __forceinline__ bool wait_counter_at_least(const unsigned int* counter, unsigned need, unsigned polls) {
+  unsigned spins = 0;
+  while (*(const volatile unsigned int*)counter < need) {
+    if (++spins > polls) return false;
+    __nanosleep(128);
+  }
+  return true;
+}
+
 // ---- warp helpers ------------------------------------------------------------------------------
 __device__ __forceinline__ uint32_t warp_inclusive_sum(uint32_t v) {
   const int lane = threadIdx.x & 31;

@@ -11,10 +11,14 @@
 //
 // Limits and rules:
 //   - The arena is kNoAllocArenaBytes = 64 MiB per GPU, declared below as a file-scope
-//     `static __device__` array: every GPU on which this library is loaded holds it until the
-//     process exits, whether or not the entry point is ever called.
+//     `static __device__` array. The driver commits it when it loads this file's device code: at
+//     the first call on a device under lazy module loading (CUDA_MODULE_LOADING=LAZY, the default
+//     since CUDA 12.2), or when the library's device code is loaded under EAGER. A caller whose
+//     device memory is fully committed later should make one warm-up call while the 64 MiB is still
+//     free. From then on every GPU that ran the entry point holds the arena until the process exits.
 //   - A call whose worst-case need exceeds the arena is rejected with SJ_ERR_INVALID before any
-//     GPU work (about 1M build rows and a few million probe rows fit; the exact need is printed).
+//     GPU work (the exact need is in the message). At load factor 0.5: 2^19 build rows with up to
+//     1.9M probe rows, or 2^20 build rows with up to 600K probe rows.
 //   - Radix partitioning and attached payloads are not used (the table is built unpartitioned).
 //   - All calls share the arena and leave their data in it; each call re-initialises everything it
 //     reads (slots, counters, offsets) before use, so stale contents never leak into a result.
@@ -25,6 +29,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -79,20 +84,35 @@ static void bump_free(void*, void*, size_t, sj_stream_t) {}
 
 static size_t a256(size_t b) { return (std::max<size_t>(b, 16) + 255) & ~(size_t)255; }
 
-// Worst case over slot encodings and layouts of what build + probe take from the allocator.
+// Buckets of a table of `keys` keys with `spb` slots per bucket at load factor lf: the same
+// power-of-two geometry build_table chooses.
+static size_t buckets_for(int64_t keys, double lf, int spb) {
+  const double slots = std::max(1.0, (double)std::max<int64_t>(keys, 1) / lf);
+  const size_t want = (size_t)std::ceil(slots / spb);
+  size_t b = 1;
+  while (b < want) b <<= 1;
+  return b;
+}
+
+// Worst case over slot encodings and layouts of what build + probe take from the allocator. The
+// bump allocator never reuses memory within a call, so every request counts, temporaries included.
 static size_t noalloc_need(int64_t n_build, int64_t n_probe, double lf) {
-  const double keys = (double)std::max<int64_t>(n_build, 1) / lf;
-  size_t buckets = 1;
-  while ((double)buckets * 2.0 < keys) buckets <<= 1;  // wide slots: 2 per bucket (more buckets)
-  const size_t slot_bytes = buckets * 32;
-  const size_t nslots = buckets * 4;
-  size_t need = a256(64);                         // build statistics
-  need += 2 * a256(slot_bytes);                   // slots + the shrunken copy of a grouped build
-  need += a256((nslots + 1) * 4) + a256((nslots + 2) * 4);  // group counts + offsets
-  need += a256((size_t)std::max<int64_t>(n_build, 1) * 4);  // grouped row positions
-  need += a256(8192);                             // scan block sums
-  const size_t np = (size_t)std::max<int64_t>(n_probe, 1);
-  need += a256(3 * a256(np * 4) + a256((np + 1) * 8) + 8192 + 256);  // grouped probe match list
+  const size_t nb = (size_t)std::max<int64_t>(n_build, 1), np = (size_t)std::max<int64_t>(n_probe, 1);
+  // Both slot encodings have the same slot count (wide: 2 per bucket; packed: 4 per bucket in half
+  // as many buckets); wide slots take the most bytes.
+  const size_t wide_buckets = buckets_for((int64_t)nb, lf, 2);
+  const size_t slot_bytes = wide_buckets * 32;
+  const size_t nslots = wide_buckets * 2;
+  size_t need = a256(sizeof(long long) * 6) + a256(slot_bytes);  // build statistics, slots
+  // grouped layout: counts + offsets over every slot, or a shrink to at most a quarter of the
+  // buckets (the copy, then counts + offsets over its slots), whichever is larger
+  const size_t groups_full = a256((nslots + 1) * 4) + a256((nslots + 2) * 4);
+  const size_t groups_shrunk = a256(slot_bytes / 4) + a256((nslots / 4 + 1) * 4) + a256((nslots / 4 + 2) * 4);
+  need += std::max(groups_full, groups_shrunk) + a256(1024 * 8);  // + the scan's block sums
+  // group members and NULL-key row ids (together at most one per build row), the NULL-row counter
+  need += a256(nb * 4) + 256 + a256(8);
+  // probe: the grouped match list in one request (a DISTINCT probe takes a 256-byte tile counter)
+  need += a256(3 * a256(np * 4) + a256((np + 1) * 8) + 1024 * 8 + 256);
   return need;
 }
 
@@ -111,15 +131,18 @@ extern "C" SJ_EXPORT sj_status sj_inner_join_noalloc(
     return set_error(SJ_ERR_INVALID, "build_keys, probe_keys and d_count are required");
   sj_join_params p;
   sj_default_params(&p);
+  // every field is honoured except partition_bits (always -1 here) and probe_partition_mb, which
+  // only applies to partitioned tables; zero fields take their defaults, as in sj_build
   if (params) {
-    p.layout = params->layout;
-    p.null_equality = params->null_equality;
-    if (params->load_factor > 0.0f) p.load_factor = params->load_factor;
-    p.force_wide = params->force_wide;
-    if (params->ctas_per_sm > 0) p.ctas_per_sm = params->ctas_per_sm;
-    p.aggregation = params->aggregation;
+    const sj_join_params defaults = p;
+    p = *params;
+    if (!(p.load_factor > 0.0f)) p.load_factor = defaults.load_factor;
+    if (p.block_size <= 0) p.block_size = defaults.block_size;
+    if (p.group_width <= 0) p.group_width = defaults.group_width;
+    if (p.ctas_per_sm <= 0) p.ctas_per_sm = defaults.ctas_per_sm;
   }
   p.partition_bits = -1;  // unpartitioned: no row store, no partition buffers
+  p.probe_partition_mb = 0;
   if (!(p.load_factor > 0.0f && p.load_factor < 1.0f)) return set_error(SJ_ERR_INVALID, "load_factor must be in (0, 1)");
   const size_t need = noalloc_need(build_keys->num_rows, probe_keys->num_rows, p.load_factor);
   if (need > kNoAllocArenaBytes)

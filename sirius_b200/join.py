@@ -329,6 +329,29 @@ def inner_join(build_keys, probe_keys, build_validity=None, probe_validity=None,
                               stream=stream).trimmed()
 
 
+# The RIGHT family of STANDARD mode (src/op/sirius_physical_hash_join.cpp:1879-1895), which the
+# reference runs with the sides swapped: RIGHT = cudf::left_join(right_keys, left_keys); RIGHT_SEMI /
+# RIGHT_ANTI = a filtered join built on the left keys and probed by the right ones.
+JOIN_RIGHT, JOIN_RIGHT_SEMI, JOIN_RIGHT_ANTI = "right", "right_semi", "right_anti"
+
+
+def right_join(kind: str, left_keys, right_keys, left_validity=None, right_validity=None, left_payload=(),
+               right_payload=(), **table_kwargs) -> JoinOutput:
+    """RIGHT / RIGHT_SEMI / RIGHT_ANTI: a table built on the LEFT keys, probed by the RIGHT keys.
+
+    The result is the swapped join's: ``probe_rid`` / ``probe_payload`` are right-side rows and
+    columns; for RIGHT, ``build_rid`` is the left row (``SJ_NO_ROW`` where the right row has no
+    match) and ``build_payload`` the left columns, NULL where unmatched. RIGHT_SEMI / RIGHT_ANTI
+    return the right rows with / without a match (a NULL right key has none). Synchronizes."""
+    inner = {JOIN_RIGHT: L.SJ_JOIN_LEFT, JOIN_RIGHT_SEMI: L.SJ_JOIN_SEMI, JOIN_RIGHT_ANTI: L.SJ_JOIN_ANTI}
+    if kind not in inner:
+        raise ValueError(f"unknown RIGHT-family join {kind!r}")
+    stream = table_kwargs.pop("stream", None)
+    with HashTable(left_keys, left_validity, stream=stream, **table_kwargs) as t:
+        return t.probe_join(inner[kind], right_keys, right_validity, right_payload,
+                            left_payload if kind == JOIN_RIGHT else (), stream=stream)
+
+
 def _host_column(data: torch.Tensor, validity: Optional[torch.Tensor] = None) -> L.SjColumn:
     """A column in host memory for sj_inner_join_host (pinned memory lets its copies overlap)."""
     if data.dim() != 1 or not data.is_contiguous() or data.is_cuda:

@@ -1,4 +1,6 @@
-"""GPU parity of LEFT / SEMI / ANTI / MARK / FULL (``sj_probe_join``) against the CPU oracle:
+"""GPU parity of LEFT / SEMI / ANTI / MARK / FULL (``sj_probe_join``) and of the RIGHT family
+(``join.right_join``: the sides swapped, as the reference's STANDARD mode runs RIGHT / RIGHT_SEMI /
+RIGHT_ANTI) against the CPU oracle:
 the reference's own known answers (NULL fixture and the MARK operator cases), then seeded inputs
 over DISTINCT and GROUPED tables, int32 and int64 keys, partitioned and unpartitioned tables,
 NULL keys on both sides and NULL payloads — row ids bit-exact after a canonical sort, gathered
@@ -167,3 +169,47 @@ def test_full_rejects_attached_payloads(cuda):
     with J.HashTable(dev_t(bk, cuda), attach=[dev_t(bk, cuda)]) as t:
         with pytest.raises(L.SjError):
             t.probe_join(L.SJ_JOIN_FULL, dev_t(bk, cuda), attached=True)
+
+
+def test_right_join_known_answer(cuda):
+    """RIGHT JOIN of the NULL fixture (test_gpu_execution_join_nulls.cpp:67-72): every right row,
+    with its left matches or a NULL left side."""
+    fx = GOLDEN["nulls_fixture"]
+    lk, lv = _col(fx["l"]["k"])
+    rk, rv = _col(fx["r"]["k"])
+    lid = np.array(fx["l"]["id"], np.int32)
+    rid = np.array(fx["r"]["id"], np.int32)
+    out = J.right_join(J.JOIN_RIGHT, dev_t(lk, cuda), dev_t(rk, cuda), dev_valid(lv, cuda), dev_valid(rv, cuda),
+                       [dev_t(lid, cuda)], [dev_t(rid, cuda)])
+    n = out.count
+    r_rows = out.probe_rid[:n].cpu().numpy()
+    l_rows = out.build_rid[:n].cpu().numpy()
+    l_ids = out.build_payload[0][:n].cpu().numpy()
+    l_ok = _bits(out.build_payload_validity[0], n)
+    got = [((int(l_ids[i]) if l_ok[i] else None), int(rid[r_rows[i]])) for i in range(n)]
+    assert all((l_rows[i] == L.SJ_NO_ROW) == (not l_ok[i]) for i in range(n))
+    key = lambda r: tuple((0, 0) if x is None else (1, x) for x in r)  # noqa: E731
+    assert sorted(got, key=key) == sorted([tuple(r) for r in fx["right"]], key=key)
+    # RIGHT_SEMI / RIGHT_ANTI: right rows with / without a left match
+    semi = J.right_join(J.JOIN_RIGHT_SEMI, dev_t(lk, cuda), dev_t(rk, cuda), dev_valid(lv, cuda), dev_valid(rv, cuda))
+    anti = J.right_join(J.JOIN_RIGHT_ANTI, dev_t(lk, cuda), dev_t(rk, cuda), dev_valid(lv, cuda), dev_valid(rv, cuda))
+    assert sorted(rid[semi.probe_rid[:semi.count].cpu().numpy()].tolist()) == [1, 2, 3]
+    assert sorted(rid[anti.probe_rid[:anti.count].cpu().numpy()].tolist()) == [4, 5]
+
+
+@pytest.mark.parametrize("kind", [J.JOIN_RIGHT, J.JOIN_RIGHT_SEMI, J.JOIN_RIGHT_ANTI])
+@pytest.mark.parametrize("dup", [False, True])
+def test_right_family_matches_oracle(cuda, kind, dup):
+    rng = np.random.default_rng(31 + dup)
+    n_l, n_r = 50_000, 300_000
+    lk = (rng.integers(0, n_l // 4, n_l) if dup else rng.permutation(n_l)).astype(np.int64) * 3 + 5
+    rk = rng.integers(0, n_l + n_l // 5, n_r).astype(np.int64) * 3 + 5
+    lv = O.pack_validity(rng.random(n_l) > 0.03)
+    rv = O.pack_validity(rng.random(n_r) > 0.05)
+    lp = rng.integers(-2**31, 2**31 - 1, n_l).astype(np.int32)
+    rp = rng.integers(-2**40, 2**40, n_r).astype(np.int64)
+    out = J.right_join(kind, dev_t(lk, cuda), dev_t(rk, cuda), dev_valid(lv, cuda), dev_valid(rv, cuda),
+                       [dev_t(lp, cuda)] if kind == J.JOIN_RIGHT else (), [dev_t(rp, cuda)])
+    # the swapped join: left is the build side, right the probe side
+    inner = {J.JOIN_RIGHT: "left", J.JOIN_RIGHT_SEMI: "semi", J.JOIN_RIGHT_ANTI: "anti"}[kind]
+    _check_rows(inner, out, lk, rk, lv, rv, [lp] if kind == J.JOIN_RIGHT else [], [rp])

@@ -963,7 +963,7 @@ void probe_runs(const sj_table* t, const void* keys, const RunArgs& ra_in, const
   a.tile_ctr = tile_ctr;
   a.l2_last = t->params.table_l2_priority == SJ_L2_EVICT_LAST;
   if (ra.n_tiles == 0) return;
-  KernelTimer timer("probe_direct", s);
+  KernelTimer timer("probe_runs", s);
   const bool wide = t->slot_kind == SJ_SLOT_WIDE128;
   if (t->key_type == SJ_INT32) {
     if (wide) launch_runs<int32_t, true>(t, keys, ra, a, s);

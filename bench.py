@@ -75,6 +75,11 @@ def parse():
     ap.add_argument("--group-width", type=int, default=0)
     ap.add_argument("--tile-rows", type=int, default=0)
     ap.add_argument("--load-factor", type=float, default=0.0)
+    ap.add_argument("--no-secondary", action="store_true",
+                    help="large workload: skip the small / skewed / batched / served records")
+    ap.add_argument("--check-joins", type=int, default=64, help="batched: joins checked row by row against the oracle")
+    ap.add_argument("--check-requests", type=int, default=16,
+                    help="served: requests checked row by row against the oracle")
     return ap.parse_args()
 
 
@@ -429,12 +434,45 @@ def run_sj(args):
             "gpu_launches": len(kernel_times),
             "clocks": clocks,
         }
-        print(json.dumps(line), flush=True)
     table.close()
+    if rank == 0 and world == 1 and not args.no_secondary:
+        # the other configurations, each with its own clocks and oracle check
+        del out, d_count, bk, pk, bp, pp, inp
+        if args.e2e_steps > 0:
+            del h_bk, h_pk, h_bp, h_pp, h_out, h_res
+        torch.cuda.synchronize()
+        torch.cuda.empty_cache()
+        line["workloads"] = run_secondary(args)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
     return 0
+
+
+def run_secondary(args):
+    """Records of the small, skewed, batched and served workloads (default sizes and seeds)."""
+    import copy
+    import torch
+    recs = {}
+    for wl in ("small", "skewed", "batched", "served"):
+        a = copy.copy(args)
+        a.workload = wl
+        a.n_build = a.n_probe = None
+        a.partition_bits, a.probe_partition_mb, a.table_l2 = 0, 0, 0
+        a.steps = 10 if wl in ("small", "skewed") else 5
+        a.autotune = wl == "batched"
+        t0 = time.perf_counter()
+        try:
+            rec = run_batched(a) if wl == "batched" else run_served(a) if wl == "served" else run_other(a)
+            rec["bench_seconds"] = round(time.perf_counter() - t0, 1)
+        except Exception as e:  # one workload's failure is reported in its record, the line still prints
+            rec = {"error": f"{type(e).__name__}: {e}"}
+        recs[wl] = rec
+        torch.cuda.synchronize()
+        torch.cuda.empty_cache()
+    return recs
 
 
 # --------------------------------------------------------------------------------------------
@@ -462,9 +500,11 @@ def batched_wave_specs(sizes, first, dev, seed):
 
 
 def run_batched(args):
+    import ctypes
     import torch
     from sirius_b200 import batch as B
     from sirius_b200 import datagen as D
+    from sirius_b200 import join as J
     from sirius_b200 import _lib
     torch.cuda.set_device(0)
     dev = torch.device("cuda", 0)
@@ -492,9 +532,15 @@ def run_batched(args):
     if cur:
         waves.append(cur)
     stream = torch.cuda.Stream()
-    t_graph = t_launch = t_per_join = 0.0
+    t_graph = t_launch = t_per_join = t_inner_each = 0.0
     probe_rows = build_rows = matches = 0
     kernels = {}
+    from oracle import oracle as O
+    O.build()
+    check_set = set(np.random.default_rng(args.seed + 5).choice(len(sizes), min(args.check_joins, len(sizes)),
+                                                                 replace=False).tolist())
+    checked_joins = checked_rows = 0
+    lib = _lib.load()
     with ClockSampler(0) as clk:
         for w in waves:
             specs = batched_wave_specs(sizes[w], w[0], dev, args.seed)
@@ -519,11 +565,47 @@ def run_batched(args):
                 counts, err = plan.counts(stream)
                 stream.synchronize()
                 assert int(err.item()) == 0 and torch.equal(counts, expect), "batched join counts differ"
+                # sampled joins of the graph-replay output against the oracle, row by row
+                for k, j in enumerate(w):
+                    if j not in check_set:
+                        continue
+                    sp, c = specs[k], int(counts[k].item())
+                    o = sp.out
+                    got = [o.probe_rid[:c].cpu().numpy(), o.build_rid[:c].cpu().numpy(),
+                           o.probe_payload[:c].cpu().numpy(), o.build_payload[:c].cpu().numpy()]
+                    ref = O.hash_join(sp.build_key.cpu().numpy(), sp.probe_key.cpu().numpy(),
+                                      probe_payload=[sp.probe_payload.cpu().numpy()],
+                                      build_payload=[sp.build_payload.cpu().numpy()])
+                    want = [ref.probe_rid, ref.build_rid, ref.probe_payload[0], ref.build_payload[0]]
+                    assert ref.rows == c, f"join {j}: {c} rows, oracle {ref.rows}"
+                    for g, e in zip(O.canonical(*got), O.canonical(*want)):
+                        assert np.array_equal(g, e), f"join {j}: rows differ from the oracle"
+                    checked_joins += 1
+                    checked_rows += c
                 t_launch += timed(lambda: plan.launch(stream), max(1, args.steps // 2))
                 t_per_join += timed(lambda: plan.launch_per_join(stream), max(1, args.steps // 4))
                 counts, err = plan.counts(stream)
                 stream.synchronize()
                 assert int(err.item()) == 0 and torch.equal(counts, expect), "per-join counts differ"
+                # what the operator calls per join today: the one-shot sj_inner_join (build, probe,
+                # gather), one call per join into the same outputs
+                d_cnt = torch.zeros(len(specs), dtype=torch.int64, device=dev)
+                cols = [(J.make_column(sp.build_key), J.make_column(sp.probe_key),
+                         J._cols([J.make_column(sp.probe_payload)]), J._cols([J.make_column(sp.build_payload)]),
+                         J._cols([J._mut(sp.out.probe_payload, None)], _lib.SjMutColumn),
+                         J._cols([J._mut(sp.out.build_payload, None)], _lib.SjMutColumn)) for sp in specs]
+
+                def inner_each():
+                    for k, sp in enumerate(specs):
+                        bc, pc, pin, bin_, pout, bout = cols[k]
+                        _lib.check(lib.sj_inner_join(ctypes.byref(bc), ctypes.byref(pc), 1, pin, 1, bin_, 1,
+                                                     sp.out.probe_rid.data_ptr(), sp.out.build_rid.data_ptr(), pout,
+                                                     bout, sp.capacity, None, None, stream.cuda_stream,
+                                                     d_cnt[k:k + 1].data_ptr()), "sj_inner_join")
+
+                t_inner_each += timed(inner_each, 1)
+                stream.synchronize()
+                assert torch.equal(d_cnt, expect), "per-join sj_inner_join counts differ"
                 probe_rows += sum(int(s.probe_key.numel()) for s in specs)
                 build_rows += sum(int(s.build_key.numel()) for s in specs)
                 matches += int(counts.sum().item())
@@ -546,10 +628,15 @@ def run_batched(args):
         "persistent_launch_ms": round(t_launch, 3), "graph_replay_ms": round(t_graph, 3),
         "one_launch_per_join_ms": round(t_per_join, 3),
         "speedup_vs_per_join": round(t_per_join / t_graph, 3),
+        "sj_inner_join_per_join_ms": round(t_inner_each, 3),
+        "speedup_vs_sj_inner_join_per_join": round(t_inner_each / t_graph, 3),
+        "oracle_check": {"kind": "per-join match counts of every join; every output row of a seeded sample of "
+                                 "joins, bit-exact after a canonical sort",
+                         "joins_counted": len(sizes), "joins_checked": checked_joins, "rows_checked": checked_rows,
+                         "passed": True},
         "gpu_launches": len(waves), "clocks": clk.summary(),
     }
-    print(json.dumps(line), flush=True)
-    return 0
+    return line
 
 
 # --------------------------------------------------------------------------------------------
@@ -585,13 +672,15 @@ def run_served(args):
     probe_rows = int(sizes.sum())
     torch.cuda.synchronize()
 
-    def make(slots):
-        srv = S.JoinServer(slots=slots, memory_budget_bytes=120 << 30, reserve_bytes=args.reserve_gib << 30)
+    def make(slots, batch):
+        srv = S.JoinServer(slots=slots, memory_budget_bytes=120 << 30, reserve_bytes=args.reserve_gib << 30,
+                           batch_small=batch)
         tids = [srv.add_table(k, attach=[p]) for k, p in tables]
         return srv, tids
 
-    def run(srv, tids, arrivals, base_id):
-        """Submit every request at t0 + arrivals[i]; returns {i: (latency s, count)}, makespan s."""
+    def run(srv, tids, arrivals, base_id, keep=None):
+        """Submit every request at t0 + arrivals[i]; returns {i: (latency s, count)}, makespan s.
+        keep: {request index: None} filled with host copies of those requests' output rows."""
         n = len(reqs)
         err = []
 
@@ -616,6 +705,9 @@ def run_served(args):
             for r in srv.poll(256, wait_ms=20):
                 assert r.status == 0, f"request {r.request_id} failed with status {r.status}"
                 got[r.request_id - base_id] = (r.t_done - r.t_submit, r.count, r.t_submit, r.t_done)
+                if keep is not None and r.request_id - base_id in keep:
+                    keep[r.request_id - base_id] = (r.probe_rid.cpu().numpy(), r.build_rid.cpu().numpy(),
+                                                    r.build_payload[0].cpu().numpy())
                 srv.release(r.request_id)
         th.join()
         if err:
@@ -625,13 +717,16 @@ def run_served(args):
 
     results = {}
     with ClockSampler(0) as clk:
-        ser, ser_t = make(1)
-        con, con_t = make(args.slots)
+        ser, ser_t = make(1, False)  # serial one-at-a-time execution: one slot, no batching
+        con, con_t = make(args.slots, True)
         # warm-up: one untimed saturated pass per server (kernels loaded, memory pools grown)
         run(ser, ser_t, None, 10_000_000)
         run(con, con_t, None, 20_000_000)
         s_sat, s_span = run(ser, ser_t, None, 0)
-        c_sat, c_span = run(con, con_t, None, 100_000)
+        sample = np.random.default_rng(args.seed + 9).choice(len(reqs), min(args.check_requests, len(reqs)),
+                                                            replace=False)
+        kept = {int(i): None for i in sample}
+        c_sat, c_span = run(con, con_t, None, 100_000, keep=kept)
         for i in range(len(reqs)):
             assert s_sat[i][1] == c_sat[i][1], f"request {i}: serial and concurrent counts differ"
         cap = len(reqs) / s_span  # serial capacity, requests/s
@@ -649,7 +744,36 @@ def run_served(args):
                              "serial_p50_ms": round(_pct(lat(s_p), 50), 3), "serial_p99_ms": round(_pct(lat(s_p), 99), 3),
                              "served_p50_ms": round(_pct(lat(c_p), 50), 3), "served_p99_ms": round(_pct(lat(c_p), 99), 3)}
         con.close()
+        # the same slots without batching the small requests: what batching adds
+        nob, nob_t = make(args.slots, False)
+        run(nob, nob_t, None, 30_000_000)
+        n_sat, n_span = run(nob, nob_t, None, 400_000)
+        arr = np.cumsum(gaps) / (0.95 * cap)
+        arr -= arr[0]
+        n_p, _ = run(nob, nob_t, arr, 500_000)
+        for i in range(len(reqs)):
+            assert n_sat[i][1] == n_p[i][1] == s_sat[i][1], f"request {i}: counts differ without batching"
+        no_batch = {"makespan_s": round(n_span, 4), "value": round(probe_rows / n_span / 1e6, 3),
+                    "poisson_0.95_p50_ms": round(_pct([v[0] * 1e3 for v in n_p.values()], 50), 3),
+                    "poisson_0.95_p99_ms": round(_pct([v[0] * 1e3 for v in n_p.values()], 99), 3)}
+        nob.close()
         ser.close()
+    # sampled requests of the saturated concurrent run against the oracle, row by row
+    from oracle import oracle as O
+    O.build()
+    host_tables = {}
+    checked_rows = 0
+    for i, rows_out in sorted(kept.items()):
+        t, pk = reqs[i]
+        if t not in host_tables:
+            host_tables[t] = (tables[t][0].cpu().numpy(), tables[t][1].cpu().numpy())
+        tk, tp = host_tables[t]
+        ref = O.hash_join(tk, pk.cpu().numpy(), build_payload=[tp])
+        assert ref.rows == len(rows_out[0]), f"request {i}: {len(rows_out[0])} rows, oracle {ref.rows}"
+        for g, e in zip(O.canonical(*rows_out), O.canonical(ref.probe_rid, ref.build_rid, ref.build_payload[0])):
+            assert np.array_equal(g, e), f"request {i}: rows differ from the oracle"
+        checked_rows += ref.rows
+    del host_tables
     matches = sum(v[1] for v in s_sat.values())
     line = {
         "metric": "served join stream: probe Mtuples/s at saturation, p50/p99 request latency",
@@ -669,10 +793,15 @@ def run_served(args):
                       "served_p50_ms": round(_pct([v[0] * 1e3 for v in c_sat.values()], 50), 3),
                       "served_p99_ms": round(_pct([v[0] * 1e3 for v in c_sat.values()], 99), 3)},
         "poisson": {str(k): v for k, v in results.items()},
+        "served_without_batching": no_batch,
+        "small_request_rows": "< 65,536 probe rows: batched into shared launches",
         "clocks": clk.summary(),
+        "oracle_check": {"kind": "match counts of every request, identical serial and concurrent, in every "
+                                 "arrival pattern; every output row of a seeded sample of requests, bit-exact "
+                                 "after a canonical sort",
+                         "requests_checked": len(kept), "rows_checked": checked_rows, "passed": True},
     }
-    print(json.dumps(line), flush=True)
-    return 0
+    return line
 
 
 # --------------------------------------------------------------------------------------------
@@ -755,20 +884,36 @@ def run_other(args):
     ktot = sum(v[1] for v in per_kernel.values()) or 1.0
     kernels = {n: {"launches": c, "ms_per_launch": round(t / c, 4), "share": round(t / ktot, 4)}
                for n, (c, t) in sorted(per_kernel.items(), key=lambda kv: -kv[1][1])}
-    cpu = None
+    from oracle import oracle as O
+    O.build()
+    threads = O.default_threads()
+    cpu, ref = None, None
     if not args.no_cpu and args.cpu_steps > 0:
-        from oracle import oracle as O
-        O.build()
-        threads = O.default_threads()
         ts = []
         for _ in range(args.cpu_steps):
             t0 = time.perf_counter()
-            r = O.hash_join(inp.build_keys, inp.probe_keys, None, inp.probe_validity, probe_payload=inp.probe_payload,
-                            build_payload=inp.build_payload, threads=threads, capacity=m)
+            ref = O.hash_join(inp.build_keys, inp.probe_keys, None, inp.probe_validity, probe_payload=inp.probe_payload,
+                              build_payload=inp.build_payload, threads=threads, capacity=m)
             ts.append(time.perf_counter() - t0)
-            assert r.rows == m
+            assert ref.rows == m
         cpu = {"value": round(inp.n_probe / statistics.median(ts) / 1e6, 3), "unit": "Mtuples/s", "cores": threads,
                "kind": "port", "sample": f"full workload, {len(ts)} one-shot CPU joins, median {statistics.median(ts):.3f} s"}
+    # the timed output against the oracle: every row (small) or the multiset checksum of every row
+    if ref is None:
+        ref = O.hash_join(inp.build_keys, inp.probe_keys, None, inp.probe_validity, probe_payload=inp.probe_payload,
+                          build_payload=inp.build_payload, threads=threads, capacity=m)
+    got = [out.probe_rid[:m].cpu().numpy(), out.build_rid[:m].cpu().numpy()] + \
+        [c[:m].cpu().numpy() for c in out.probe_payload] + [c[:m].cpu().numpy() for c in out.build_payload]
+    want = [ref.probe_rid, ref.build_rid] + list(ref.probe_payload) + list(ref.build_payload)
+    if args.workload == "small":
+        for g, e in zip(O.canonical(*got), O.canonical(*want)):
+            assert np.array_equal(g, e), "small: output rows differ from the oracle"
+        check = {"kind": "every output row, bit-exact after a canonical sort", "rows": m, "passed": True}
+    else:
+        assert O.multiset_checksum(*got) == O.multiset_checksum(*want), "skewed: output checksum differs"
+        check = {"kind": "64-bit order-independent checksum of every output row (probe rid, build rid, payloads)",
+                 "rows": m, "passed": True}
+    del got, want, ref
     desc = (f"small: build {inp.n_build} unique int32 keys (permutation) + int32 payload; probe {inp.n_probe} "
             f"int32 keys uniform over 1.1x the build range + int32 payload" if args.workload == "small" else
             f"skewed: build {inp.n_build} int64 keys Zipf(1.1) over 1M values + int32 payload; probe {inp.n_probe} "
@@ -787,9 +932,9 @@ def run_other(args):
                      "frac": round(achieved / peak, 4), "traffic": None, "alg_bytes_per_launch": int(alg),
                      "launch_ms": round(ms, 4), "kernels": kernels, "peak_source": peak_src},
         "cpu_baseline": cpu, "gpu_launches": len(kt), "clocks": clk.summary(),
+        "oracle_check": check,
     }
-    print(json.dumps(line), flush=True)
-    return 0
+    return line
 
 
 def main():
@@ -799,12 +944,10 @@ def main():
         args.n_probe = args.n_probe or 64 << 20
     if args.impl == "reference":
         return run_reference(args)
-    if args.workload == "batched":
-        return run_batched(args)
-    if args.workload == "served":
-        return run_served(args)
-    if args.workload in ("small", "skewed"):
-        return run_other(args)
+    if args.workload in ("batched", "served", "small", "skewed"):
+        runner = {"batched": run_batched, "served": run_served}.get(args.workload, run_other)
+        print(json.dumps(runner(args)), flush=True)
+        return 0
     return run_sj(args)
 
 

@@ -430,7 +430,12 @@ typedef struct sj_server_config {
   int64_t memory_budget_bytes;  /* device bytes for request outputs + scratch; default 120 GiB */
   int64_t reserve_bytes;        /* device memory the server's pool takes up front and keeps, so
                                    requests are served without growing it; default 0 */
-  int32_t reserved[6];
+  int32_t batch_small;          /* 0 (default): requests of fewer than 65,536 rows into tables whose
+                                   attached payloads are 8-byte fields without NULLs (at most 3)
+                                   are batched: all such queued requests run as one kernel launch
+                                   on the server's batch stream while it is idle; -1: every request
+                                   runs alone on a slot stream */
+  int32_t reserved[5];
 } sj_server_config;
 
 /* A finished request. Output buffers are device memory owned by the server until

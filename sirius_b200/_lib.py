@@ -78,7 +78,7 @@ class SjKernelTime(Structure):
 
 class SjServerConfig(Structure):
     _fields_ = [("slots", c_int32), ("max_skip", c_int32), ("memory_budget_bytes", c_int64),
-                ("reserve_bytes", c_int64), ("reserved", c_int32 * 6)]
+                ("reserve_bytes", c_int64), ("batch_small", c_int32), ("reserved", c_int32 * 5)]
 
 
 class SjRequestResult(Structure):

@@ -14,6 +14,12 @@
 //     server's own stream-ordered memory pool) while others run on theirs, so requests that
 //     arrive while earlier ones are on the GPU start as soon as a slot and memory free up and
 //     their work overlaps on the device;
+//   - small requests (fewer rows than a partitioned probe takes) are batched continuously: while
+//     the batch stream is idle, the worker admits every queued small request that fits (up to 256)
+//     as ONE launch of the multi-request probe kernel (sj_serve_batch.cu) on its own stream — one
+//     descriptor upload, one kernel, one count copy and one host callback for all of them — while
+//     large requests keep running on the slot streams; requests that arrive meanwhile form the
+//     next batch;
 //   - a host callback after the request's last GPU operation stamps its completion time; the
 //     worker then returns its scratch charge and hands it to poll(); release() frees its outputs
 //     (the caller must have finished reading them, e.g. synchronized its own stream).
@@ -33,6 +39,7 @@
 
 #include "sj_internal.h"
 #include "sj_partition.cuh"
+#include "sj_serve_batch.h"
 
 namespace sj {
 
@@ -70,8 +77,9 @@ struct SrvReq {
   int32_t* brid = nullptr;
   void* bpay[8] = {};
   uint32_t* bval[8] = {};
-  int slot = -1;
+  int slot = -1;   // slot stream, or -1 in the batch
   int skipped = 0;
+  bool batchable = false;
   sj_status status = SJ_OK;
 };
 
@@ -88,6 +96,17 @@ struct sj_server {
   std::deque<sj::SrvReq*> finished;
   std::unordered_map<uint64_t, sj::SrvReq*> polled;
   size_t in_use = 0;
+  // the batch of small requests: its stream, the requests in flight and their device descriptors
+  // and counts (pinned host copies)
+  cudaStream_t batch_stream = nullptr;
+  std::vector<sj::SrvReq*> batch;
+  bool batch_busy = false;
+  std::atomic<int> batch_done{0};
+  sj::ServeReq* h_reqs = nullptr;
+  sj::ServeReq* d_reqs = nullptr;
+  unsigned long long* d_counts = nullptr;
+  int64_t* h_counts = nullptr;
+  unsigned* d_item_ctr = nullptr;
   std::mutex mu;
   std::condition_variable cv_work, cv_done;
   std::thread worker;
@@ -180,6 +199,55 @@ static void run_request(sj_server* S, SrvReq* r) {
   }
 }
 
+static void CUDART_CB on_batch_done(void* p) {
+  sj_server* S = static_cast<sj_server*>(p);
+  std::lock_guard<std::mutex> lk(S->mu);
+  const double t = now_s();
+  for (SrvReq* r : S->batch) r->t_done.store(t);
+  S->batch_done.store(1);
+  S->cv_work.notify_one();
+}
+
+// Enqueue the admitted batch of small requests on the batch stream (called without the lock held).
+static void run_batch(sj_server* S) {
+  cudaStream_t s = S->batch_stream;
+  const sj_alloc a{S, pool_alloc, pool_free};
+  const Allocator alloc(&a);
+  int n = 0;
+  for (size_t i = 0; i < S->batch.size(); ++i) {
+    SrvReq* r = S->batch[i];
+    const SrvTable& T = r->tab;
+    const int64_t rows = r->key.num_rows;
+    sj_status st = alloc.allocate((void**)&r->prid, a256((size_t)rows * 4), s);
+    if (st == SJ_OK) st = alloc.allocate((void**)&r->brid, a256((size_t)rows * 4), s);
+    for (int c = 0; c < T.n_payload && st == SJ_OK; ++c) st = alloc.allocate(&r->bpay[c], a256((size_t)rows * 8), s);
+    r->status = st;
+    if (st != SJ_OK) continue;  // reported by the completion pass; its outputs are freed there
+    S->h_reqs[n] = serve_request(T.t, r->key, r->prid, r->brid, r->bpay, S->d_counts + i);
+    ++n;
+  }
+  sj_status st = SJ_OK;
+  if (cudaMemsetAsync(S->d_counts, 0, sizeof(unsigned long long) * S->batch.size(), s) != cudaSuccess)
+    st = SJ_ERR_DEVICE;
+  if (st == SJ_OK && n > 0) st = serve_batch_launch(S->h_reqs, n, S->d_reqs, S->d_item_ctr, S->device, s);
+  if (st == SJ_OK && cudaMemcpyAsync(S->h_counts, S->d_counts, 8 * S->batch.size(), cudaMemcpyDeviceToHost, s) !=
+                         cudaSuccess)
+    st = SJ_ERR_DEVICE;
+  if (st != SJ_OK)
+    for (SrvReq* r : S->batch)
+      if (r->status == SJ_OK) r->status = st;
+  if (st != SJ_OK || cudaLaunchHostFunc(s, on_batch_done, S) != cudaSuccess) {
+    cudaStreamSynchronize(s);
+    std::lock_guard<std::mutex> lk(S->mu);
+    const double t = now_s();
+    for (SrvReq* r : S->batch) {
+      if (r->status == SJ_OK) r->status = SJ_ERR_DEVICE;
+      r->t_done.store(t);
+    }
+    S->batch_done.store(1);
+  }
+}
+
 static void free_outputs(sj_server* S, SrvReq* r, cudaStream_t s) {
   auto give = [&](void* p) {
     if (p) cudaFreeAsync(p, s);
@@ -220,24 +288,56 @@ static void worker_loop(sj_server* S) {
       S->finished.push_back(r);
       S->cv_done.notify_all();
     }
+    if (S->batch_busy) {
+      if (!S->batch_done.load()) {
+        busy = true;
+      } else {
+        for (size_t i = 0; i < S->batch.size(); ++i) {
+          SrvReq* r = S->batch[i];
+          r->count = r->status == SJ_OK ? S->h_counts[i] : 0;
+          S->in_use -= r->scratch_bytes;
+          if (r->status != SJ_OK) {
+            free_outputs(S, r, S->batch_stream);
+            S->in_use -= r->out_bytes;
+            r->out_bytes = 0;
+          }
+          S->finished.push_back(r);
+        }
+        S->batch.clear();
+        S->batch_busy = false;
+        S->batch_done.store(0);
+        S->cv_done.notify_all();
+      }
+    }
     // admission: FIFO; smaller requests may pass a head that does not fit, boundedly
     std::vector<SrvReq*> admit, ahead;  // ahead: queued requests passed over in this sweep
+    const bool batch_open = S->cfg.batch_small >= 0 && !S->batch_busy;
     for (auto it = S->pending.begin(); it != S->pending.end();) {
-      int free_slot = -1;
-      for (size_t i = 0; i < S->slots.size(); ++i)
-        if (!S->slots[i].req) {
-          free_slot = (int)i;
-          break;
-        }
-      if (free_slot < 0) break;
       SrvReq* r = *it;
+      // a small request joins the batch being formed while the batch stream is idle; any other
+      // request needs a free slot stream
+      const bool to_batch = batch_open && r->batchable && S->batch.size() < (size_t)kServeMaxBatch;
+      int free_slot = -1;
+      if (!to_batch) {
+        for (size_t i = 0; i < S->slots.size(); ++i)
+          if (!S->slots[i].req) {
+            free_slot = (int)i;
+            break;
+          }
+        if (free_slot < 0) break;
+      }
       const size_t need = r->out_bytes + r->scratch_bytes;
       if (S->in_use + need <= (size_t)S->cfg.memory_budget_bytes) {
         S->in_use += need;
-        r->slot = free_slot;
         r->t_admit = now_s();
-        S->slots[free_slot].req = r;
-        admit.push_back(r);
+        if (to_batch) {
+          r->slot = -1;
+          S->batch.push_back(r);
+        } else {
+          r->slot = free_slot;
+          S->slots[free_slot].req = r;
+          admit.push_back(r);
+        }
         it = S->pending.erase(it);
         busy = true;
         for (SrvReq* q : ahead) ++q->skipped;
@@ -247,9 +347,12 @@ static void worker_loop(sj_server* S) {
         ++it;
       }
     }
-    if (!admit.empty()) {
+    const bool launch_batch = batch_open && !S->batch.empty();
+    if (launch_batch) S->batch_busy = true;
+    if (!admit.empty() || launch_batch) {
       lk.unlock();
       for (SrvReq* r : admit) run_request(S, r);
+      if (launch_batch) run_batch(S);  // S->batch is only changed by this thread
       lk.lock();
       continue;
     }
@@ -286,6 +389,7 @@ SJ_EXPORT sj_status sj_server_create(const sj_server_config* config, sj_server**
     if (config->max_skip > 0) S->cfg.max_skip = config->max_skip;
     if (config->memory_budget_bytes > 0) S->cfg.memory_budget_bytes = config->memory_budget_bytes;
     if (config->reserve_bytes > 0) S->cfg.reserve_bytes = std::min(config->reserve_bytes, S->cfg.memory_budget_bytes);
+    S->cfg.batch_small = config->batch_small;
   }
   if (S->cfg.slots > 64) {
     delete S;
@@ -322,6 +426,15 @@ SJ_EXPORT sj_status sj_server_create(const sj_server_config* config, sj_server**
     }
     cudaFreeAsync(p, S->release_stream);
     cudaStreamSynchronize(S->release_stream);
+  }
+  if (cudaStreamCreateWithFlags(&S->batch_stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaMallocHost((void**)&S->h_reqs, sizeof(ServeReq) * kServeMaxBatch) != cudaSuccess ||
+      cudaMalloc((void**)&S->d_reqs, sizeof(ServeReq) * kServeMaxBatch) != cudaSuccess ||
+      cudaMalloc((void**)&S->d_counts, sizeof(unsigned long long) * kServeMaxBatch) != cudaSuccess ||
+      cudaMallocHost((void**)&S->h_counts, sizeof(int64_t) * kServeMaxBatch) != cudaSuccess ||
+      cudaMalloc((void**)&S->d_item_ctr, 256) != cudaSuccess) {
+    sj_server_destroy(S);
+    return set_error(SJ_ERR_DEVICE, "creating the server's batch stream failed");
   }
   S->slots.resize(S->cfg.slots);
   for (SrvSlot& sl : S->slots) {
@@ -385,6 +498,7 @@ SJ_EXPORT sj_status sj_server_submit(sj_server* S, int32_t table_id, const sj_co
     r->table = table_id;
     r->tab = S->tables[table_id];
     r->key = *probe_key;
+    r->batchable = serve_batchable(r->tab.t, probe_key->num_rows);
     size_request(S, r);
     if (r->out_bytes + r->scratch_bytes > (size_t)S->cfg.memory_budget_bytes) {
       delete r;
@@ -466,6 +580,15 @@ SJ_EXPORT sj_status sj_server_destroy(sj_server* S) {
   }
   for (SrvSlot& sl : S->slots)
     if (sl.stream) cudaStreamSynchronize(sl.stream);
+  if (S->batch_stream) {
+    cudaStreamSynchronize(S->batch_stream);
+    cudaStreamDestroy(S->batch_stream);
+  }
+  if (S->h_reqs) cudaFreeHost(S->h_reqs);
+  if (S->d_reqs) cudaFree(S->d_reqs);
+  if (S->d_counts) cudaFree(S->d_counts);
+  if (S->h_counts) cudaFreeHost(S->h_counts);
+  if (S->d_item_ctr) cudaFree(S->d_item_ctr);
   for (SrvSlot& sl : S->slots) {
     if (sl.stream) cudaStreamDestroy(sl.stream);
     if (sl.d_count) cudaFree(sl.d_count);

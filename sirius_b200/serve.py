@@ -65,12 +65,15 @@ class JoinServer:
     """Resident tables + continuous batching of probe requests (``sj_server_create``)."""
 
     def __init__(self, slots: int = 4, max_skip: int = 8, memory_budget_bytes: int = 120 << 30,
-                 reserve_bytes: int = 0, device=None):
+                 reserve_bytes: int = 0, batch_small: bool = True, device=None):
+        """``batch_small``: run queued small requests (fewer than 65,536 rows) together as one kernel
+        launch on the server's batch stream; False runs every request alone on a slot stream."""
         self._lib = L.load()
         self.device = torch.device("cuda", torch.cuda.current_device()) if device is None else torch.device(device)
         cfg = L.SjServerConfig()
         cfg.slots, cfg.max_skip, cfg.memory_budget_bytes = slots, max_skip, memory_budget_bytes
         cfg.reserve_bytes = reserve_bytes
+        cfg.batch_small = 0 if batch_small else -1
         self._h = ctypes.c_void_p()
         with torch.cuda.device(self.device):
             L.check(self._lib.sj_server_create(ctypes.byref(cfg), ctypes.byref(self._h)), "sj_server_create")

@@ -1,7 +1,8 @@
 """GPU tests of the join server: every request's result is the same alone (one request on the GPU
-at a time) and in the mix (several slots, requests admitted as slots and memory free up), and
-equal to the CPU oracle; admission under a small memory budget; requests larger than the budget
-are refused; closing a server whose queue cannot drain cancels the queued requests."""
+at a time, no batching) and in the mix (several slots, requests admitted as slots and memory free
+up, small requests batched into shared launches), and equal to the CPU oracle; small requests
+really share launches; admission under a small memory budget; requests larger than the budget are
+refused; closing a server whose queue cannot drain cancels the queued requests."""
 import numpy as np
 import pytest
 import torch
@@ -68,7 +69,7 @@ def _run(server, tids, reqs, alone):
 def test_results_identical_alone_and_in_the_mix(cuda):
     tables = _tables(cuda)
     reqs = _requests(cuda, tables, 40)
-    with S.JoinServer(slots=1) as one:
+    with S.JoinServer(slots=1, batch_small=False) as one:
         tids = [one.add_table(k, attach=[p], partition_bits=(3 if t == 2 else -1)) for t, (k, p) in enumerate(tables)]
         alone = _run(one, tids, reqs, alone=True)
     with S.JoinServer(slots=4) as many:
@@ -89,6 +90,56 @@ def test_results_identical_alone_and_in_the_mix(cuda):
         assert ref.rows == alone[i][0]
         exp = O.canonical(ref.probe_rid, ref.build_rid, ref.build_payload[0])
         for a, b in zip(alone[i][1], exp):
+            assert np.array_equal(a, b), f"request {i} differs from the oracle"
+
+
+def test_small_requests_share_launches(cuda):
+    """Hundreds of small requests (1K..60K rows) submitted at once run as a few batch launches: the
+    requests of one batch complete together (one callback stamps them all). Each result equals the
+    same request run alone without batching, and the oracle; wide (full-range int64) and packed
+    (int32 key) tables are mixed in one batch."""
+    tables = _tables(cuda)
+    k32 = torch.randperm(200_000, device=cuda, dtype=torch.int64).to(torch.int32) * 3
+    p32 = torch.randint(-2**60, 2**60, (200_000,), device=cuda, dtype=torch.int64)
+    reqs = _requests(cuda, tables, 300, seed=21, lo=1e3, hi=6e4)
+    g = torch.Generator(device=cuda)
+    g.manual_seed(4)
+    reqs += [(3, (torch.randint(0, 700_000, (int(n),), device=cuda, generator=g)).to(torch.int32))
+             for n in np.random.default_rng(5).integers(1_000, 60_000, 60)]
+    torch.cuda.synchronize()
+
+    def serve(batch):
+        with S.JoinServer(slots=4, batch_small=batch) as srv:
+            tids = [srv.add_table(k, attach=[p], partition_bits=-1) for k, p in tables]
+            tids.append(srv.add_table(k32, attach=[p32], partition_bits=-1))
+            for i, (t, pk) in enumerate(reqs):
+                srv.submit(tids[t], pk, i, sync=(i == 0))
+            got, done_at = {}, {}
+            while len(got) < len(reqs):
+                for r in srv.poll(64, wait_ms=1000):
+                    assert r.status == L.SJ_OK
+                    got[r.request_id] = (r.count, _result_rows(r))
+                    done_at[r.request_id] = r.t_done
+                    srv.release(r.request_id)
+        return got, done_at
+
+    batched, done_at = serve(True)
+    plain, _ = serve(False)
+    groups = {}
+    for i, t in done_at.items():
+        groups.setdefault(t, []).append(i)
+    assert len(groups) < len(reqs) // 4, f"{len(groups)} completion groups for {len(reqs)} requests"
+    for i in range(len(reqs)):
+        assert batched[i][0] == plain[i][0]
+        for a, b in zip(batched[i][1], plain[i][1]):
+            assert np.array_equal(a, b), f"request {i} differs batched vs alone"
+    host = [(k.cpu().numpy(), p.cpu().numpy()) for k, p in tables] + [(k32.cpu().numpy(), p32.cpu().numpy())]
+    for i in range(0, len(reqs), 11):
+        t, pk = reqs[i]
+        bk, bp = host[t]
+        ref = O.hash_join(bk, pk.cpu().numpy(), build_payload=[bp], threads=8)
+        assert ref.rows == batched[i][0]
+        for a, b in zip(batched[i][1], O.canonical(ref.probe_rid, ref.build_rid, ref.build_payload[0])):
             assert np.array_equal(a, b), f"request {i} differs from the oracle"
 
 

@@ -177,7 +177,12 @@ typedef struct sj_join_params {
                                  of the table one sweep keeps in L2); 0 = default (48) */
   int32_t table_l2_priority;  /* sj_l2_priority of the table's slot and record loads in the
                                  direct probe kernels */
-  int32_t reserved[3];
+  int32_t bloom_bits_per_key; /* > 0: the build also produces the join's dynamic filter (the
+                                 blocked Bloom filter of sj_bloom_build, that many bits per build
+                                 row), its bits set by the insert pass itself, so the filter costs no
+                                 second read of the build keys; read it with sj_table_bloom. One key
+                                 column only. 0 = none */
+  int32_t reserved[2];
 } sj_join_params;
 
 typedef struct sj_table sj_table;
@@ -341,6 +346,10 @@ SJ_EXPORT sj_status sj_bloom_build(const sj_column* keys, int32_t bits_per_key, 
 SJ_EXPORT sj_status sj_bloom_contains(const sj_bloom* bloom, const sj_column* probe_keys, uint8_t* out_mask,
                                       uint32_t* out_validity, sj_stream_t stream);
 SJ_EXPORT int64_t sj_bloom_bytes(const sj_bloom* bloom);
+/* The dynamic filter a table's build produced (sj_join_params.bloom_bits_per_key > 0), or NULL.
+ * It is the filter sj_bloom_build would make from the same key column, bit for bit; test it with
+ * sj_bloom_contains. The table owns it: it lives until sj_table_destroy (do not destroy it). */
+SJ_EXPORT const sj_bloom* sj_table_bloom(const sj_table* table);
 SJ_EXPORT sj_status sj_bloom_destroy(sj_bloom* bloom, sj_stream_t stream);
 
 /* One-shot INNER join (STANDARD mode: cudf::inner_join(left_keys, right_keys, compare_nulls(),
@@ -521,7 +530,8 @@ SJ_EXPORT sj_status sj_inner_join_host(const sj_column* build_keys, const sj_col
  * *d_count = matches). Inputs whose worst-case scratch exceeds the array are rejected with
  * SJ_ERR_INVALID before any GPU work; at load factor 0.5 that allows 2^19 build rows with up to
  * 1.9M probe rows, or 2^20 build rows with up to 600K probe rows. The table is never
- * radix-partitioned: every params field is honoured except partition_bits and probe_partition_mb.
+ * radix-partitioned and builds no dynamic filter: every params field is honoured except
+ * partition_bits, probe_partition_mb and bloom_bits_per_key.
  * All calls share the array and leave their data in it; each call re-initialises what it reads,
  * but calls that overlap on the GPU race: serialise them (one stream, or synchronise between).
  * The first call on a device looks up the array's device address (cudaGetSymbolAddress) with that

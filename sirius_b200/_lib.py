@@ -50,7 +50,7 @@ class SjJoinParams(Structure):
                 ("block_size", c_int32), ("group_width", c_int32), ("partition_bits", c_int32),
                 ("force_wide", c_int32), ("ctas_per_sm", c_int32), ("aggregation", c_int32),
                 ("probe_kernel", c_int32), ("rows_per_lane", c_int32), ("probe_partition_mb", c_int32),
-                ("table_l2_priority", c_int32), ("reserved", c_int32 * 3)]
+                ("table_l2_priority", c_int32), ("bloom_bits_per_key", c_int32), ("reserved", c_int32 * 2)]
 
 
 class SjTableInfo(Structure):
@@ -118,6 +118,7 @@ SIGNATURES = {
     "sj_bloom_build": (c_int32, [_P(SjColumn), c_int32, _P(SjAlloc), c_void_p, _P(c_void_p)]),
     "sj_bloom_contains": (c_int32, [c_void_p, _P(SjColumn), c_void_p, c_void_p, c_void_p]),
     "sj_bloom_bytes": (c_int64, [c_void_p]),
+    "sj_table_bloom": (c_void_p, [c_void_p]),
     "sj_bloom_destroy": (c_int32, [c_void_p, c_void_p]),
     "sj_status_string": (c_char_p, [c_int32]),
     "sj_last_error": (c_char_p, []),

@@ -172,6 +172,7 @@ static sj_join_params resolve(const sj_join_params* p) {
   r.rows_per_lane = p->rows_per_lane;
   r.probe_partition_mb = p->probe_partition_mb;
   r.table_l2_priority = p->table_l2_priority;
+  r.bloom_bits_per_key = p->bloom_bits_per_key;
   return r;
 }
 
@@ -206,6 +207,8 @@ SJ_EXPORT sj_status sj_build(const sj_column* keys, int32_t num_keys, const sj_j
 static sj_status build_keys(const sj_column* keys, int32_t num_keys, const sj_column* payload, int32_t num_payload,
                             const sj_join_params& p, const Allocator& a, cudaStream_t s, sj_table** out) {
   if (num_keys == 1) return build_table(keys[0], payload, num_payload, p, a, s, out);
+  if (p.bloom_bits_per_key > 0)
+    return set_error(SJ_ERR_INVALID, "a build-time dynamic filter needs a single key column");
   KeyPack kp{};
   Scratch buf;
   sj_column packed{};

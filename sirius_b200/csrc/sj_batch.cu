@@ -225,13 +225,15 @@ __device__ void probe_tile(const BatchDev& P, const BJoin& J, int32_t join, int3
 }
 
 // Group width 1: each lane keeps kBatchR probe rows in flight (rows base + 32 j + lane, so every
-// key load is one coalesced warp access). Two rows per lane (80 registers, 3 CTAs of 256 per SM)
-// beat one row (4 CTAs) by 18 % and four rows (105 registers, 2 CTAs) by 36 % on 4,096 joins. A step probes one bucket for each of the lane's live
-// rows; the matches of all its rows are reserved with one atomicAdd per warp and step. When every
-// row has at most one match in the step (unique build keys), group j's hit lanes are ranked with a
-// ballot so each output column is written as one contiguous run per group; otherwise positions
-// follow (lane, row group, slot) order. A row stops at its first bucket with an EMPTY slot (its
-// matches there still count) or once the whole table has been scanned.
+// key load is one coalesced warp access). Two rows per lane (3 CTAs of 256 per SM) beat one row
+// (4 CTAs) by 18 % and four rows (2 CTAs) by 36 % on 4,096 joins. A step probes one bucket for
+// each of the lane's live rows. When every row has at most one match in the step (unique build
+// keys), all loads a match needs are in flight before the warp reserves its output range: the
+// probe payload loads with the key, the build payload (by row id) right after the bucket match;
+// group j's hit lanes are then ranked with a ballot so each output column is written as one
+// contiguous run per group. Otherwise (duplicates in one bucket) positions follow (lane, row
+// group, slot) order. A row stops at its first bucket with an EMPTY slot (its matches there still
+// count) or once the whole table has been scanned.
 constexpr int kBatchR = 2;
 
 template <typename K>
@@ -243,15 +245,17 @@ __device__ void probe_tile_r(const BatchDev& P, const BJoin& J, int32_t join, in
   const int64_t lo = (int64_t)tile * P.tile_rows;
   const int64_t hi = min(J.np, lo + P.tile_rows);
   const uint64_t mask = (1ull << J.log2_nb) - 1;
+  const bool has_pp = J.ppay.data != nullptr, has_bp = J.bpay.data != nullptr;
   for (int64_t base = lo + (int64_t)(threadIdx.x >> 5) * 32 * R; base < hi; base += (int64_t)nwarps * 32 * R) {
     K k[R];
-    uint64_t b[R];
+    uint64_t b[R], pv[R];
     uint32_t act = 0;
 #pragma unroll
     for (int j = 0; j < R; ++j) {
       const int64_t i = base + 32 * j + lane;
       const bool live = i < hi && bit_valid(J.pvalid, J.pvoff, i);
       k[j] = live ? load_key<K>(J.pkey, i) : (K)0;
+      pv[j] = live && has_pp ? load_elem(J.ppay.data, i, J.ppay.width) : 0;  // in flight with the key
       b[j] = live ? bhome<K>(J, k[j]) : 0;
       if (live) act |= 1u << j;
     }
@@ -269,17 +273,17 @@ __device__ void probe_tile_r(const BatchDev& P, const BJoin& J, int32_t join, in
         if (has_empty || step >= mask) act &= ~(1u << j);
         else b[j] = (b[j] + 1) & mask;
       }
-      // write one match: output position p, probe row i, build row id rid
-      auto put = [&](int64_t p, int64_t i, int32_t brow) {
+      // write one match: output position p, probe row i, build row id brow, payloads
+      auto put = [&](int64_t p, int64_t i, int32_t brow, uint64_t pval, uint64_t bval) {
         if (p >= J.capacity) return;
         if (J.out_prid) J.out_prid[p] = (int32_t)i;
         if (J.out_brid) J.out_brid[p] = brow;
-        if (J.ppay.data) {
-          store_elem(J.out_ppay.data, p, J.ppay.width, load_elem(J.ppay.data, i, J.ppay.width));
+        if (has_pp) {
+          store_elem(J.out_ppay.data, p, J.ppay.width, pval);
           if (J.ppay.valid && bit_valid(J.ppay.valid, J.ppay.voff, i)) set_out_bit(J.out_ppay.valid, p);
         }
-        if (J.bpay.data) {
-          store_elem(J.out_bpay.data, p, J.bpay.width, load_elem(J.bpay.data, brow, J.bpay.width));
+        if (has_bp) {
+          store_elem(J.out_bpay.data, p, J.bpay.width, bval);
           if (J.bpay.valid && bit_valid(J.bpay.valid, J.bpay.voff, brow)) set_out_bit(J.out_bpay.valid, p);
         }
       };
@@ -287,11 +291,17 @@ __device__ void probe_tile_r(const BatchDev& P, const BJoin& J, int32_t join, in
 #pragma unroll
       for (int j = 0; j < R; ++j) single &= (m[j] & (m[j] - 1u)) == 0;
       if (__all_sync(kFullMask, single)) {
-        // row-group-major positions: group j's hit lanes write one contiguous run per column
+        // the matched build rows and their payloads first, then one reservation per warp
+        int32_t brow[R];
+        uint64_t bv[R];
         unsigned bal[R];
         uint32_t tot = 0;
 #pragma unroll
         for (int j = 0; j < R; ++j) {
+          brow[j] = 0;
+#pragma unroll
+          for (int q = 0; q < S; ++q) brow[j] = (m[j] >> q & 1u) ? rid[j][q] : brow[j];
+          bv[j] = m[j] && has_bp ? load_elem(J.bpay.data, brow[j], J.bpay.width) : 0;
           bal[j] = __ballot_sync(kFullMask, m[j] != 0);
           tot += __popc(bal[j]);
         }
@@ -302,10 +312,7 @@ __device__ void probe_tile_r(const BatchDev& P, const BJoin& J, int32_t join, in
         const unsigned below = (1u << lane) - 1u;
 #pragma unroll
         for (int j = 0; j < R; ++j) {
-          int32_t brow = 0;
-#pragma unroll
-          for (int q = 0; q < S; ++q) brow = (m[j] >> q & 1u) ? rid[j][q] : brow;
-          if (m[j]) put((int64_t)(pos + __popc(bal[j] & below)), base + 32 * j + lane, brow);
+          if (m[j]) put((int64_t)(pos + __popc(bal[j] & below)), base + 32 * j + lane, brow[j], pv[j], bv[j]);
           pos += __popc(bal[j]);
         }
       } else {
@@ -316,7 +323,9 @@ __device__ void probe_tile_r(const BatchDev& P, const BJoin& J, int32_t join, in
         for (int j = 0; j < R; ++j)
 #pragma unroll
           for (int q = 0; q < S; ++q)
-            if (m[j] >> q & 1u) put((int64_t)pos0 + r++, base + 32 * j + lane, rid[j][q]);
+            if (m[j] >> q & 1u)
+              put((int64_t)pos0 + r++, base + 32 * j + lane, rid[j][q], pv[j],
+                  has_bp ? load_elem(J.bpay.data, rid[j][q], J.bpay.width) : 0);
       }
     }
   }

@@ -3,46 +3,26 @@
 // "may contain" mask per probe row with the probe's NULLs; published by the hash join,
 // src/op/sirius_physical_hash_join.cpp:1960-2069).
 //
-// Layout: 2^log2_blocks blocks of 8 x 32-bit words (32 bytes = one DRAM sector). A key's block is
-// the top bits of mix64(key); a second mix of that hash gives 8 five-bit numbers, one bit per word.
-// Insert: 8 atomicOr on one sector; test: one 256-bit load and 8 bit tests, so a probe row costs
-// one sector read. NULL build keys are not inserted; NULL probe rows test false with a NULL mask.
+// Layout (bloom_locate, sj_device.cuh): 2^log2_blocks blocks of 8 x 32-bit words (32 bytes = one
+// DRAM sector). A key's block is the top bits of mix64(key); a second mix of that hash gives 8
+// five-bit numbers, one bit per word. Insert: 8 atomicOr on one sector; test: one 256-bit load and
+// 8 bit tests, so a probe row costs one sector read. NULL build keys are not inserted; NULL probe
+// rows test false with a NULL mask. The same filter can come out of a table's build, set by its
+// insert pass (sj_join_params.bloom_bits_per_key, sj_build.cu), instead of a second pass here.
 #include <algorithm>
 #include <string>
 
 #include "sj_device.cuh"
 #include "sj_internal.h"
 
-struct sj_bloom {
-  int device = 0;
-  sj::Allocator alloc;
-  uint32_t* words = nullptr;
-  size_t bytes = 0;
-  int32_t log2_blocks = 0;
-  int32_t key_type = SJ_INT64;
-  int64_t keys = 0;
-};
-
 namespace sj {
-
-constexpr uint64_t kBloomSalt = 0x9E3779B97F4A7C15ull;
-
-__device__ __forceinline__ void bloom_locate(uint64_t kb, int log2_blocks, uint64_t& block, uint64_t& bits) {
-  const uint64_t h = mix64(kb);
-  block = log2_blocks ? h >> (64 - log2_blocks) : 0;
-  bits = mix64(h + kBloomSalt);  // word w uses bits [5w, 5w + 5)
-}
 
 template <typename K>
 __global__ void __launch_bounds__(256) bloom_insert_kernel(const K* __restrict__ keys, const uint32_t* kv, int64_t kvoff,
                                                            int64_t n, uint32_t* words, int log2_blocks) {
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     if (!bit_valid(kv, kvoff, i)) continue;
-    uint64_t block, bits;
-    bloom_locate(key_u64<K>(__ldg(keys + i)), log2_blocks, block, bits);
-    uint32_t* b = words + block * 8;
-#pragma unroll
-    for (int w = 0; w < 8; ++w) atomicOr(b + w, 1u << ((bits >> (5 * w)) & 31));
+    bloom_add(words, log2_blocks, key_u64<K>(__ldg(keys + i)));
   }
 }
 
@@ -79,6 +59,37 @@ static int grid_of(int device, int64_t n) {
   return (int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, (int64_t)sm_count(device) * 8));
 }
 
+sj_status bloom_create(int64_t n_keys, int32_t bits_per_key, int32_t key_type, const Allocator& alloc, cudaStream_t s,
+                       sj_bloom** out) {
+  *out = nullptr;
+  if (bits_per_key <= 0) bits_per_key = 16;
+  if (bits_per_key > 1024) return set_error(SJ_ERR_INVALID, "bits_per_key must be in [1, 1024]");
+  sj_bloom* b = new sj_bloom();
+  b->alloc = alloc;
+  cudaGetDevice(&b->device);
+  b->key_type = key_type;
+  b->keys = n_keys;
+  const uint64_t want_bits = (uint64_t)std::max<int64_t>(n_keys, 1) * (uint64_t)bits_per_key;
+  while (b->log2_blocks < 40 && ((uint64_t)256 << b->log2_blocks) < want_bits) ++b->log2_blocks;
+  b->bytes = (size_t)32 << b->log2_blocks;
+  if (sj_status e = b->alloc.allocate((void**)&b->words, b->bytes, s)) {
+    delete b;
+    return e;
+  }
+  if (cudaMemsetAsync(b->words, 0, b->bytes, s) != cudaSuccess) {
+    bloom_free(b, s);
+    return set_error(SJ_ERR_DEVICE, "bloom filter memset failed");
+  }
+  *out = b;
+  return SJ_OK;
+}
+
+void bloom_free(sj_bloom* b, cudaStream_t s) {
+  if (!b) return;
+  if (b->words) b->alloc.release(b->words, b->bytes, s);
+  delete b;
+}
+
 }  // namespace sj
 
 using namespace sj;
@@ -91,26 +102,9 @@ SJ_EXPORT sj_status sj_bloom_build(const sj_column* keys, int32_t bits_per_key, 
   if (!out || !keys) return set_error(SJ_ERR_INVALID, "keys and out are required");
   *out = nullptr;
   SJ_TRY(validate_column(keys, "bloom key", true));
-  if (bits_per_key <= 0) bits_per_key = 16;
-  if (bits_per_key > 1024) return set_error(SJ_ERR_INVALID, "bits_per_key must be in [1, 1024]");
   const cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-  sj_bloom* b = new sj_bloom();
-  b->alloc = Allocator(alloc);
-  cudaGetDevice(&b->device);
-  b->key_type = keys->type;
-  b->keys = keys->num_rows;
-  const uint64_t want_bits = (uint64_t)std::max<int64_t>(keys->num_rows, 1) * (uint64_t)bits_per_key;
-  while (b->log2_blocks < 40 && ((uint64_t)256 << b->log2_blocks) < want_bits) ++b->log2_blocks;
-  b->bytes = (size_t)32 << b->log2_blocks;
-  if (sj_status e = b->alloc.allocate((void**)&b->words, b->bytes, s)) {
-    delete b;
-    return e;
-  }
-  if (cudaMemsetAsync(b->words, 0, b->bytes, s) != cudaSuccess) {
-    b->alloc.release(b->words, b->bytes, s);
-    delete b;
-    return set_error(SJ_ERR_DEVICE, "bloom filter memset failed");
-  }
+  sj_bloom* b = nullptr;
+  SJ_TRY(bloom_create(keys->num_rows, bits_per_key, keys->type, Allocator(alloc), s, &b));
   const int64_t n = keys->num_rows;
   if (n > 0) {
     KernelTimer timer("bloom_build", s);
@@ -122,8 +116,7 @@ SJ_EXPORT sj_status sj_bloom_build(const sj_column* keys, int32_t bits_per_key, 
           static_cast<const int64_t*>(keys->data), keys->validity, keys->validity_offset, n, b->words, b->log2_blocks);
   }
   if (cudaGetLastError() != cudaSuccess) {
-    b->alloc.release(b->words, b->bytes, s);
-    delete b;
+    bloom_free(b, s);
     return set_error(SJ_ERR_DEVICE, "bloom filter build launch failed");
   }
   *out = b;
@@ -156,10 +149,10 @@ SJ_EXPORT sj_status sj_bloom_contains(const sj_bloom* bloom, const sj_column* pr
 SJ_EXPORT int64_t sj_bloom_bytes(const sj_bloom* bloom) { return bloom ? (int64_t)bloom->bytes : 0; }
 
 SJ_EXPORT sj_status sj_bloom_destroy(sj_bloom* bloom, sj_stream_t stream) {
-  if (!bloom) return SJ_OK;
-  if (bloom->words) bloom->alloc.release(bloom->words, bloom->bytes, reinterpret_cast<cudaStream_t>(stream));
-  delete bloom;
+  bloom_free(bloom, reinterpret_cast<cudaStream_t>(stream));
   return SJ_OK;
 }
+
+SJ_EXPORT const sj_bloom* sj_table_bloom(const sj_table* table) { return table ? table->bloom : nullptr; }
 
 }  // extern "C"

@@ -145,10 +145,12 @@ __device__ __forceinline__ uint32_t find_slot(const TableDev& t, uint64_t kb, ui
   return 0xffffffffu;
 }
 
+// bloom != NULL: the build's dynamic filter gets each inserted key's bits in the same pass (the key
+// is already in a register; its hash is the one the insert computes).
 template <typename K, bool WIDE>
 __global__ void __launch_bounds__(256) insert_kernel(TableDev t, const K* __restrict__ keys,
                                                      const uint32_t* kv, int64_t kvoff, int64_t n,
-                                                     BuildStats* st) {
+                                                     BuildStats* st, uint32_t* bloom, int bloom_log2) {
   const int lane = threadIdx.x & 31;
   for (int64_t i0 = (int64_t)blockIdx.x * blockDim.x; i0 < n; i0 += (int64_t)gridDim.x * blockDim.x) {
     const int64_t i = i0 + threadIdx.x;
@@ -159,6 +161,7 @@ __global__ void __launch_bounds__(256) insert_kernel(TableDev t, const K* __rest
       const uint64_t kn = (uint64_t)(long long)k - (uint64_t)t.kmin;
       uint32_t s;
       r = insert_or_find<WIDE>(t, kb, kn, (int32_t)i, &s);
+      if (bloom) bloom_add(bloom, bloom_log2, kb);
     }
     const unsigned dup = __ballot_sync(kFullMask, r == 1);
     const unsigned full = __ballot_sync(kFullMask, r == 2);
@@ -344,9 +347,11 @@ static void launch_stats(const sj_column& c, int grid, BuildStats* st, cudaStrea
 }
 
 template <typename K, bool WIDE>
-static void launch_insert(const TableDev& d, const sj_column& c, int grid, BuildStats* st, cudaStream_t s) {
+static void launch_insert(const TableDev& d, const sj_column& c, int grid, BuildStats* st, sj_bloom* bloom,
+                          cudaStream_t s) {
   insert_kernel<K, WIDE><<<grid, 256, 0, s>>>(d, static_cast<const K*>(c.data), c.validity,
-                                              c.validity_offset, c.num_rows, st);
+                                              c.validity_offset, c.num_rows, st, bloom ? bloom->words : nullptr,
+                                              bloom ? bloom->log2_blocks : 0);
 }
 
 template <typename K, bool WIDE>
@@ -423,6 +428,8 @@ sj_status build_table(const sj_column& keys, const sj_column* payload, int32_t n
     return set_error(SJ_ERR_INVALID, "probe_partition_mb must be in [0, 65536]");
   if (p.table_l2_priority < SJ_L2_AUTO || p.table_l2_priority > SJ_L2_EVICT_LAST)
     return set_error(SJ_ERR_INVALID, "unknown table_l2_priority");
+  if (p.bloom_bits_per_key < 0 || p.bloom_bits_per_key > 1024)
+    return set_error(SJ_ERR_INVALID, "bloom_bits_per_key must be in [0, 1024]");
   if (n_payload < 0 || n_payload > kMaxPayload || (n_payload > 0 && payload == nullptr))
     return set_error(SJ_ERR_INVALID, "at most 8 attached payload columns");
   for (int c = 0; c < n_payload; ++c) {
@@ -574,10 +581,14 @@ sj_status build_table(const sj_column& keys, const sj_column* payload, int32_t n
   const int64_t sn = src.num_rows;
   const int sgrid = grid_for(t->device, p, std::max<int64_t>(sn, 1), 256);
 
+  // the dynamic filter, sized by the build rows as sj_bloom_build sizes it, filled by the insert
+  if (p.bloom_bits_per_key > 0)
+    if (sj_status e = bloom_create(n, p.bloom_bits_per_key, keys.type, alloc, stream, &t->bloom)) return fail(e);
   TableDev d = make_dev(t);
   if (t->valid_rows > 0) {
+    KernelTimer timer("insert", stream);
     by_type(keys.type, wide, [&](auto k, auto w) {
-      launch_insert<decltype(k), decltype(w)::value>(d, src, sgrid, st, stream);
+      launch_insert<decltype(k), decltype(w)::value>(d, src, sgrid, st, t->bloom, stream);
     });
   }
   if (cudaMemcpyAsync(&h, st, sizeof(h), cudaMemcpyDeviceToHost, stream) != cudaSuccess ||
@@ -682,6 +693,7 @@ sj_status destroy_table(sj_table* t, cudaStream_t stream) {
   if (t->grp_rid) t->alloc.release(t->grp_rid, t->grp_rid_bytes, stream);
   if (t->arow) t->alloc.release(t->arow, t->arow_bytes, stream);
   if (t->null_rid) t->alloc.release(t->null_rid, t->null_rid_bytes, stream);
+  bloom_free(t->bloom, stream);
   if (t->apay_owned) {
     for (int c = 0; c < t->n_attached; ++c) {
       if (t->apay[c]) t->alloc.release(t->apay[c], t->apay_bytes[c], stream);

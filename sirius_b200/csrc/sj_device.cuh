@@ -269,6 +269,26 @@ __device__ __forceinline__ bool bit_valid(const uint32_t* v, int64_t off, int64_
   return (__ldg(v + (b >> 5)) >> (b & 31)) & 1u;
 }
 
+// ---- blocked Bloom filter ----------------------------------------------------------------------
+// 2^log2_blocks blocks of 8 x 32-bit words (32 bytes = one DRAM sector). A key's block is the top
+// bits of mix64(key) (the table's hash); a second mix of that hash gives 8 five-bit numbers, one
+// bit per word.
+constexpr uint64_t kBloomSalt = 0x9E3779B97F4A7C15ull;
+
+__device__ __forceinline__ void bloom_locate(uint64_t kb, int log2_blocks, uint64_t& block, uint64_t& bits) {
+  const uint64_t h = mix64(kb);
+  block = log2_blocks ? h >> (64 - log2_blocks) : 0;
+  bits = mix64(h + kBloomSalt);  // word w uses bits [5w, 5w + 5)
+}
+
+__device__ __forceinline__ void bloom_add(uint32_t* words, int log2_blocks, uint64_t kb) {
+  uint64_t block, bits;
+  bloom_locate(kb, log2_blocks, block, bits);
+  uint32_t* b = words + block * 8;
+#pragma unroll
+  for (int w = 0; w < 8; ++w) atomicOr(b + w, 1u << ((bits >> (5 * w)) & 31));
+}
+
 // ---- bounded waits -----------------------------------------------------------------------------
 // Polls `*counter` (written by other CTAs) until it reaches `need`, sleeping ~128 ns between polls;
 // gives up after `polls` polls and returns false. One thread calls it; the caller publishes the

@@ -99,6 +99,16 @@ struct KeyPack {
 };
 }  // namespace sj
 
+struct sj_bloom {
+  int device = 0;
+  sj::Allocator alloc;
+  uint32_t* words = nullptr;
+  size_t bytes = 0;
+  int32_t log2_blocks = 0;
+  int32_t key_type = SJ_INT64;
+  int64_t keys = 0;
+};
+
 struct sj_table {
   int device = 0;
   sj::Allocator alloc;
@@ -145,6 +155,7 @@ struct sj_table {
   // join emits them as unmatched rows). Built only when the build has NULL keys.
   int32_t* null_rid  = nullptr;
   size_t null_rid_bytes = 0;
+  sj_bloom* bloom    = nullptr;  // the dynamic filter set by the insert pass (bloom_bits_per_key > 0)
   size_t apay_bytes[8] = {};
   size_t apay_valid_bytes[8] = {};
   sj_join_params params{};
@@ -194,6 +205,11 @@ sj_status pack_probe_keys(const KeyPack& kp, const sj_column* keys, int n_keys, 
 // Hash partitioning of a table (sj_partition_op.cu).
 sj_status hash_partition(const sj_column* keys, int n_keys, const sj_column* cols, int n_cols, int n_parts,
                          const sj_mut_column* out, int64_t* d_offsets, const Allocator& alloc, cudaStream_t s);
+
+// Blocked Bloom filter of n keys at `bits_per_key` (sj_bloom.cu): words allocated and zeroed on `s`.
+sj_status bloom_create(int64_t n_keys, int32_t bits_per_key, int32_t key_type, const Allocator& alloc, cudaStream_t s,
+                       sj_bloom** out);
+void bloom_free(sj_bloom* b, cudaStream_t s);
 
 // LEFT / SEMI / ANTI / MARK / FULL (sj_probe_kinds.cu); INNER delegates to probe_gather.
 sj_status probe_join(const sj_table* t, int32_t kind, const sj_column& probe, const GatherSpec& g, uint8_t* out_mark,

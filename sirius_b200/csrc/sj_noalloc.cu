@@ -131,8 +131,9 @@ extern "C" SJ_EXPORT sj_status sj_inner_join_noalloc(
     return set_error(SJ_ERR_INVALID, "build_keys, probe_keys and d_count are required");
   sj_join_params p;
   sj_default_params(&p);
-  // every field is honoured except partition_bits (always -1 here) and probe_partition_mb, which
-  // only applies to partitioned tables; zero fields take their defaults, as in sj_build
+  // every field is honoured except partition_bits (always -1 here), probe_partition_mb, which only
+  // applies to partitioned tables, and bloom_bits_per_key (the table is discarded at the end of the
+  // call); zero fields take their defaults, as in sj_build
   if (params) {
     const sj_join_params defaults = p;
     p = *params;
@@ -143,6 +144,7 @@ extern "C" SJ_EXPORT sj_status sj_inner_join_noalloc(
   }
   p.partition_bits = -1;  // unpartitioned: no row store, no partition buffers
   p.probe_partition_mb = 0;
+  p.bloom_bits_per_key = 0;  // no dynamic filter: it would outlive the call
   if (!(p.load_factor > 0.0f && p.load_factor < 1.0f)) return set_error(SJ_ERR_INVALID, "load_factor must be in (0, 1)");
   const size_t need = noalloc_need(build_keys->num_rows, probe_keys->num_rows, p.load_factor);
   if (need > kNoAllocArenaBytes)

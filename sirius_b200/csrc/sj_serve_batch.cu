@@ -4,7 +4,7 @@
 //
 // A batch is a list of request descriptors, each naming its own resident table (by value: the
 // TableDev view plus its row store), its probe keys and its own outputs and match counter. Work
-// items are 1024-row slices of the requests, numbered request after request; a warp takes the next
+// items are 256-row slices of the requests, numbered request after request; a warp takes the next
 // item from a counter, finds its request with a binary search over the requests' first items
 // (held in shared memory), and probes the slice in steps of 32 x R rows exactly as the direct
 // DISTINCT probe does: lane l handles rows base + 32 j + l, one bucket walk per row, one row-store
@@ -21,7 +21,7 @@ namespace sj {
 
 TableDev table_dev(const sj_table* t);
 
-constexpr int kItemRows = 1024;
+constexpr int kItemRows = 256;  // rows per work item: a 30K-row request spreads over ~120 warps
 constexpr int kServeThreads = 256;
 constexpr int kServeR = 2;
 

@@ -93,6 +93,7 @@ struct sj_server {
   std::vector<sj::SrvTable> tables;
   std::vector<sj::SrvSlot> slots;
   std::deque<sj::SrvReq*> pending;
+  size_t pending_small = 0;  // queued requests that may join a batch
   std::deque<sj::SrvReq*> finished;
   std::unordered_map<uint64_t, sj::SrvReq*> polled;
   size_t in_use = 0;
@@ -312,19 +313,33 @@ static void worker_loop(sj_server* S) {
     // admission: FIFO; smaller requests may pass a head that does not fit, boundedly
     std::vector<SrvReq*> admit, ahead;  // ahead: queued requests passed over in this sweep
     const bool batch_open = S->cfg.batch_small >= 0 && !S->batch_busy;
+    bool slots_full = false;  // a queued request found no free slot: later ones may only join the batch
     for (auto it = S->pending.begin(); it != S->pending.end();) {
       SrvReq* r = *it;
-      // a small request joins the batch being formed while the batch stream is idle; any other
-      // request needs a free slot stream
+      // a small request joins the batch being formed while the batch stream is idle (passing large
+      // requests that wait for a slot: its work is a few microseconds); any other request needs a
+      // free slot stream, in queue order
       const bool to_batch = batch_open && r->batchable && S->batch.size() < (size_t)kServeMaxBatch;
       int free_slot = -1;
       if (!to_batch) {
+        // with every slot busy, only batchable requests can still be admitted in this sweep
+        const bool may_batch = batch_open && S->pending_small > 0 && S->batch.size() < (size_t)kServeMaxBatch;
+        if (slots_full) {
+          if (!may_batch) break;
+          ++it;
+          continue;
+        }
         for (size_t i = 0; i < S->slots.size(); ++i)
           if (!S->slots[i].req) {
             free_slot = (int)i;
             break;
           }
-        if (free_slot < 0) break;
+        if (free_slot < 0) {
+          slots_full = true;
+          if (!may_batch) break;
+          ++it;
+          continue;
+        }
       }
       const size_t need = r->out_bytes + r->scratch_bytes;
       if (S->in_use + need <= (size_t)S->cfg.memory_budget_bytes) {
@@ -338,6 +353,7 @@ static void worker_loop(sj_server* S) {
           S->slots[free_slot].req = r;
           admit.push_back(r);
         }
+        if (r->batchable) --S->pending_small;
         it = S->pending.erase(it);
         busy = true;
         for (SrvReq* q : ahead) ++q->skipped;
@@ -364,6 +380,7 @@ static void worker_loop(sj_server* S) {
         S->finished.push_back(r);
       }
       S->pending.clear();
+      S->pending_small = 0;
       break;
     }
     S->cv_work.wait_for(lk, std::chrono::microseconds(200));
@@ -506,6 +523,7 @@ SJ_EXPORT sj_status sj_server_submit(sj_server* S, int32_t table_id, const sj_co
     }
     r->t_submit = now_s();
     S->pending.push_back(r);
+    if (r->batchable) ++S->pending_small;
   }
   S->cv_work.notify_one();
   return SJ_OK;

@@ -142,10 +142,12 @@ class HashTable:
                  ctas_per_sm: int = 0, aggregation: int = L.SJ_AGG_AUTO,
                  probe_kernel: int = L.SJ_PROBE_KERNEL_AUTO, rows_per_lane: int = 0,
                  probe_partition_mb: int = 0, table_l2_priority: int = L.SJ_L2_AUTO,
-                 stream: Optional[torch.cuda.Stream] = None):
+                 bloom_bits_per_key: int = 0, stream: Optional[torch.cuda.Stream] = None):
         """Build the table. ``attach``: build payload columns (tensor or (tensor, validity)) the
         table copies in its own position order (sj_build_ex); gather them with
-        ``probe_gather(..., attached=True)``. ``partition_bits``: 0 = automatic, -1 = never."""
+        ``probe_gather(..., attached=True)``. ``partition_bits``: 0 = automatic, -1 = never.
+        ``bloom_bits_per_key`` > 0: the insert pass also fills the join's dynamic filter
+        (``bloom()``)."""
         self._lib = L.load()
         self._handle = ctypes.c_void_p()
         self.keys = keys
@@ -153,7 +155,8 @@ class HashTable:
                                        partition_bits=partition_bits, force_wide=int(force_wide),
                                        aggregation=aggregation, probe_kernel=probe_kernel,
                                        rows_per_lane=rows_per_lane, probe_partition_mb=probe_partition_mb,
-                                       table_l2_priority=table_l2_priority)
+                                       table_l2_priority=table_l2_priority,
+                                       bloom_bits_per_key=bloom_bits_per_key)
         if ctas_per_sm:
             self.params.ctas_per_sm = ctas_per_sm
         col, nkeys, first = _keys(keys, validity)
@@ -174,6 +177,11 @@ class HashTable:
         if not self._handle:
             raise RuntimeError("table is closed")
         return self._handle
+
+    def bloom(self) -> Optional["BloomFilter"]:
+        """The dynamic filter the build filled (``bloom_bits_per_key`` > 0), owned by the table."""
+        h = self._lib.sj_table_bloom(self.handle)
+        return BloomFilter.view(h, self) if h else None
 
     def info(self) -> L.SjTableInfo:
         inf = L.SjTableInfo()
@@ -442,9 +450,19 @@ class BloomFilter:
                  stream: Optional[torch.cuda.Stream] = None):
         self._lib = L.load()
         self._h = ctypes.c_void_p()
+        self._owner = None
         col = make_column(keys, validity)
         L.check(self._lib.sj_bloom_build(ctypes.byref(col), bits_per_key, None, _stream_handle(stream),
                                          ctypes.byref(self._h)), "sj_bloom_build")
+
+    @classmethod
+    def view(cls, handle: int, owner) -> "BloomFilter":
+        """A filter owned by `owner` (a HashTable's build-time filter): never destroyed here."""
+        b = cls.__new__(cls)
+        b._lib = L.load()
+        b._h = ctypes.c_void_p(handle)
+        b._owner = owner
+        return b
 
     @property
     def nbytes(self) -> int:
@@ -463,9 +481,9 @@ class BloomFilter:
         return mask, valid
 
     def close(self):
-        if self._h:
+        if self._h and self._owner is None:
             self._lib.sj_bloom_destroy(self._h, None)
-            self._h = ctypes.c_void_p()
+        self._h = ctypes.c_void_p()
 
     def __enter__(self):
         return self

@@ -77,6 +77,13 @@ __device__ __forceinline__ K load_key(const void* base, int64_t i) {
 }
 
 // ---- table access for one join ------------------------------------------------------------------
+// Bucket b of the arena in one 32-byte load through L2 (.cg: the same launch's build items wrote the
+// bucket with atomics, so it must not come from a stale L1 line).
+__device__ __forceinline__ void load_bucket_cg(const void* arena, uint64_t b, uint64_t (&s)[4]) {
+  const unsigned long long* p = reinterpret_cast<const unsigned long long*>(arena) + b * 4;
+  asm volatile("ld.global.cg.v4.u64 {%0, %1, %2, %3}, [%4];" : "=l"(s[0]), "=l"(s[1]), "=l"(s[2]), "=l"(s[3]) : "l"(p));
+}
+
 template <typename K>
 struct BTable;
 
@@ -101,9 +108,8 @@ struct BTable<int32_t> {  // 4 x uint64 (key << 32 | rid) per bucket
   // matches of key k in bucket b (bits), and whether the bucket has an EMPTY slot
   __device__ __forceinline__ static uint32_t probe(const void* arena, uint64_t b, int32_t k, bool& has_empty,
                                                    int32_t (&rid)[4]) {
-    const ulonglong2* q = reinterpret_cast<const ulonglong2*>(arena) + b * 2;
-    const ulonglong2 x = __ldcg(q), y = __ldcg(q + 1);
-    const uint64_t s[4] = {x.x, x.y, y.x, y.y};
+    uint64_t s[4];
+    load_bucket_cg(arena, b, s);
     uint32_t m = 0;
     has_empty = false;
 #pragma unroll
@@ -137,23 +143,36 @@ struct BTable<int64_t> {  // 2 x {key, rid} per bucket
   }
   __device__ __forceinline__ static uint32_t probe(const void* arena, uint64_t b, int64_t k, bool& has_empty,
                                                    int32_t (&rid)[4]) {
-    const ulonglong2* q = reinterpret_cast<const ulonglong2*>(arena) + b * 2;
-    const ulonglong2 x = __ldcg(q), y = __ldcg(q + 1);
+    uint64_t s[4];
+    load_bucket_cg(arena, b, s);
     uint32_t m = 0;
-    const bool e0 = x.y == kEmpty, e1 = y.y == kEmpty;
+    const bool e0 = s[1] == kEmpty, e1 = s[3] == kEmpty;
     has_empty = e0 || e1;
-    if (!e0 && (int64_t)x.x == k) m |= 1u;
-    if (!e1 && (int64_t)y.x == k) m |= 2u;
-    rid[0] = (int32_t)x.y;
-    rid[1] = (int32_t)y.y;
+    if (!e0 && (int64_t)s[0] == k) m |= 1u;
+    if (!e1 && (int64_t)s[2] == k) m |= 2u;
+    rid[0] = (int32_t)s[1];
+    rid[1] = (int32_t)s[3];
     rid[2] = rid[3] = 0;
     return m;
   }
 };
 
+// The home bucket of a key in its join's table. The batch's tables are built and probed only by
+// this file, so int32 keys take a 32-bit mixer: the finalizer of MurmurHash3 (Austin Appleby,
+// public domain; a bijection on 32 bits), about a third of the 64-bit mixer's instructions.
+__device__ __forceinline__ uint32_t fmix32(uint32_t h) {
+  h ^= h >> 16;
+  h *= 0x85ebca6bu;
+  h ^= h >> 13;
+  h *= 0xc2b2ae35u;
+  h ^= h >> 16;
+  return h;
+}
+
 template <typename K>
 __device__ __forceinline__ uint64_t bhome(const BJoin& J, K k) {
-  return J.log2_nb ? (mix64(key_u64<K>(k)) >> (64 - J.log2_nb)) : 0;
+  if constexpr (sizeof(K) == 4) return J.log2_nb ? (fmix32((uint32_t)k) >> (32 - J.log2_nb)) : 0;
+  else return J.log2_nb ? (mix64(key_u64<K>(k)) >> (64 - J.log2_nb)) : 0;
 }
 
 // ---- work items ---------------------------------------------------------------------------------
@@ -236,7 +255,16 @@ __device__ void probe_tile(const BatchDev& P, const BJoin& J, int32_t join, int3
 // count) or once the whole table has been scanned.
 constexpr int kBatchR = 2;
 
-template <typename K>
+// SH = 4 or 8: every join of the plan gathers one probe and one build payload of SH bytes without
+// NULLs and writes both row ids (typed loads and stores, no per-store checks); 0: read from J.
+template <int SH>
+__device__ __forceinline__ uint64_t pay_load(const PayloadIn& in, int64_t i) {
+  if constexpr (SH == 8) return __ldg(static_cast<const unsigned long long*>(in.data) + i);
+  else if constexpr (SH == 4) return __ldg(static_cast<const unsigned int*>(in.data) + i);
+  else return load_elem(in.data, i, in.width);
+}
+
+template <typename K, int SH>
 __device__ void probe_tile_r(const BatchDev& P, const BJoin& J, int32_t join, int32_t tile) {
   constexpr int S = BTable<K>::kSlots;
   constexpr int R = kBatchR;
@@ -245,7 +273,7 @@ __device__ void probe_tile_r(const BatchDev& P, const BJoin& J, int32_t join, in
   const int64_t lo = (int64_t)tile * P.tile_rows;
   const int64_t hi = min(J.np, lo + P.tile_rows);
   const uint64_t mask = (1ull << J.log2_nb) - 1;
-  const bool has_pp = J.ppay.data != nullptr, has_bp = J.bpay.data != nullptr;
+  const bool has_pp = SH || J.ppay.data != nullptr, has_bp = SH || J.bpay.data != nullptr;
   for (int64_t base = lo + (int64_t)(threadIdx.x >> 5) * 32 * R; base < hi; base += (int64_t)nwarps * 32 * R) {
     K k[R];
     uint64_t b[R], pv[R];
@@ -255,7 +283,7 @@ __device__ void probe_tile_r(const BatchDev& P, const BJoin& J, int32_t join, in
       const int64_t i = base + 32 * j + lane;
       const bool live = i < hi && bit_valid(J.pvalid, J.pvoff, i);
       k[j] = live ? load_key<K>(J.pkey, i) : (K)0;
-      pv[j] = live && has_pp ? load_elem(J.ppay.data, i, J.ppay.width) : 0;  // in flight with the key
+      pv[j] = live && has_pp ? pay_load<SH>(J.ppay, i) : 0;  // in flight with the key
       b[j] = live ? bhome<K>(J, k[j]) : 0;
       if (live) act |= 1u << j;
     }
@@ -276,6 +304,18 @@ __device__ void probe_tile_r(const BatchDev& P, const BJoin& J, int32_t join, in
       // write one match: output position p, probe row i, build row id brow, payloads
       auto put = [&](int64_t p, int64_t i, int32_t brow, uint64_t pval, uint64_t bval) {
         if (p >= J.capacity) return;
+        if constexpr (SH != 0) {
+          __stcs(J.out_prid + p, (int32_t)i);
+          __stcs(J.out_brid + p, brow);
+          if constexpr (SH == 8) {
+            __stcs(static_cast<unsigned long long*>(J.out_ppay.data) + p, (unsigned long long)pval);
+            __stcs(static_cast<unsigned long long*>(J.out_bpay.data) + p, (unsigned long long)bval);
+          } else {
+            __stcs(static_cast<unsigned int*>(J.out_ppay.data) + p, (unsigned int)pval);
+            __stcs(static_cast<unsigned int*>(J.out_bpay.data) + p, (unsigned int)bval);
+          }
+          return;
+        }
         if (J.out_prid) J.out_prid[p] = (int32_t)i;
         if (J.out_brid) J.out_brid[p] = brow;
         if (has_pp) {
@@ -301,7 +341,7 @@ __device__ void probe_tile_r(const BatchDev& P, const BJoin& J, int32_t join, in
           brow[j] = 0;
 #pragma unroll
           for (int q = 0; q < S; ++q) brow[j] = (m[j] >> q & 1u) ? rid[j][q] : brow[j];
-          bv[j] = m[j] && has_bp ? load_elem(J.bpay.data, brow[j], J.bpay.width) : 0;
+          bv[j] = m[j] && has_bp ? pay_load<SH>(J.bpay, brow[j]) : 0;
           bal[j] = __ballot_sync(kFullMask, m[j] != 0);
           tot += __popc(bal[j]);
         }
@@ -325,7 +365,7 @@ __device__ void probe_tile_r(const BatchDev& P, const BJoin& J, int32_t join, in
           for (int q = 0; q < S; ++q)
             if (m[j] >> q & 1u)
               put((int64_t)pos0 + r++, base + 32 * j + lane, rid[j][q], pv[j],
-                  has_bp ? load_elem(J.bpay.data, rid[j][q], J.bpay.width) : 0);
+                  has_bp ? pay_load<SH>(J.bpay, rid[j][q]) : 0);
       }
     }
   }
@@ -339,8 +379,10 @@ __device__ __forceinline__ void wait_built(const BatchDev& P, int32_t join, int3
   __syncthreads();
 }
 
-template <typename K, int G>
-__global__ void batch_persistent_kernel(BatchDev P) {
+// 64 registers at most: four CTAs of 256 threads per SM (the shape-specialised probe needs 66
+// otherwise, which leaves three)
+template <typename K, int G, int SH>
+__global__ void __launch_bounds__(512, 2) batch_persistent_kernel(BatchDev P) {
   __shared__ long long s_item;
   for (;;) {
     if (threadIdx.x == 0) s_item = (long long)atomicAdd(P.queue, 1ull);
@@ -359,7 +401,7 @@ __global__ void batch_persistent_kernel(BatchDev P) {
       }
     } else {
       wait_built(P, item.join, J.build_tiles);
-      if constexpr (G == 1) probe_tile_r<K>(P, J, item.join, item.tile);
+      if constexpr (G == 1) probe_tile_r<K, SH>(P, J, item.join, item.tile);
       else probe_tile<K, G>(P, J, item.join, item.tile);
     }
   }
@@ -371,11 +413,11 @@ __global__ void batch_build_one_kernel(BatchDev P, int32_t j) {
   const BJoin J = P.joins[j];
   for (int32_t t = blockIdx.x; t < J.build_tiles; t += gridDim.x) build_tile<K>(P, J, t);
 }
-template <typename K, int G>
+template <typename K, int G, int SH>
 __global__ void batch_probe_one_kernel(BatchDev P, int32_t j, int32_t probe_tiles) {
   const BJoin J = P.joins[j];
   for (int32_t t = blockIdx.x; t < probe_tiles; t += gridDim.x) {
-    if constexpr (G == 1) probe_tile_r<K>(P, J, j, t);
+    if constexpr (G == 1) probe_tile_r<K, SH>(P, J, j, t);
     else probe_tile<K, G>(P, J, j, t);
   }
 }
@@ -391,6 +433,7 @@ struct sj_batch_plan {
   sj_batch_params params{};
   int32_t key_type = SJ_INT32;
   int32_t n_joins = 0;
+  int32_t shape = 0;  // compile-time output shape of the probe (4 / 8: see probe_tile_r), or 0
   std::vector<sj::BJoin> host_joins;
   std::vector<int32_t> probe_tiles;
   sj::BatchDev dev{};
@@ -434,21 +477,24 @@ static sj_status batch_resolve(const sj_batch_params* in, sj_batch_params& p) {
   return SJ_OK;
 }
 
+// key type x group width x output shape (the compile-time shape only with group width 1)
 template <typename F>
-static void dispatch_kg(int32_t key_type, int g, F&& f) {
-#define SJ_G(K)                                      \
-  switch (g) {                                       \
-    case 1: f(K{}, std::integral_constant<int, 1>{}); break; \
-    case 2: f(K{}, std::integral_constant<int, 2>{}); break; \
-    case 4: f(K{}, std::integral_constant<int, 4>{}); break; \
-    default: f(K{}, std::integral_constant<int, 8>{}); break; \
-  }
-  if (key_type == SJ_INT32) {
-    SJ_G(int32_t)
-  } else {
-    SJ_G(int64_t)
-  }
-#undef SJ_G
+static void dispatch_kg(int32_t key_type, int g, int shape, F&& f) {
+  using I1 = std::integral_constant<int, 1>;
+  auto go = [&](auto k) {
+    switch (g) {
+      case 1:
+        if (shape == 8) f(k, I1{}, std::integral_constant<int, 8>{});
+        else if (shape == 4) f(k, I1{}, std::integral_constant<int, 4>{});
+        else f(k, I1{}, std::integral_constant<int, 0>{});
+        break;
+      case 2: f(k, std::integral_constant<int, 2>{}, std::integral_constant<int, 0>{}); break;
+      case 4: f(k, std::integral_constant<int, 4>{}, std::integral_constant<int, 0>{}); break;
+      default: f(k, std::integral_constant<int, 8>{}, std::integral_constant<int, 0>{}); break;
+    }
+  };
+  if (key_type == SJ_INT32) go(int32_t{});
+  else go(int64_t{});
 }
 
 static sj_status reset_batch(sj_batch_plan* P, cudaStream_t s) {
@@ -460,8 +506,9 @@ static sj_status reset_batch(sj_batch_plan* P, cudaStream_t s) {
 static int resident_ctas(sj_batch_plan* P) {
   int per_sm = 0;
   const int block = P->params.block_size;
-  dispatch_kg(P->key_type, P->params.group_width, [&](auto k, auto g) {
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_persistent_kernel<decltype(k), decltype(g)::value>,
+  dispatch_kg(P->key_type, P->params.group_width, P->shape, [&](auto k, auto g, auto sh) {
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm,
+                                                  batch_persistent_kernel<decltype(k), decltype(g)::value, decltype(sh)::value>,
                                                   block, 0);
   });
   per_sm = std::max(1, std::min(per_sm, P->params.ctas_per_sm));
@@ -547,6 +594,17 @@ SJ_EXPORT sj_status sj_batch_plan_create(const sj_batch_join* joins, int32_t n, 
     P->probe_tiles.push_back(pt);
     P->host_joins.push_back(J);
   }
+  // one compile-time output shape when every join gathers both payloads of one width (4 or 8 bytes)
+  // without NULLs and writes both row ids
+  int shape = -1;
+  for (const BJoin& J : P->host_joins) {
+    const int w = J.ppay.data && J.bpay.data && J.ppay.width == J.bpay.width && !J.ppay.valid && !J.bpay.valid &&
+                          J.out_prid && J.out_brid
+                      ? J.ppay.width
+                      : 0;
+    shape = shape < 0 ? w : (shape == w ? w : 0);
+  }
+  P->shape = shape == 4 || shape == 8 ? shape : 0;
   // if any join's clear is needed, memset covers all slices; the layout is fixed by the plan
   P->arena_bytes = (size_t)std::max<int64_t>(buckets, 1) * kBucketBytes;
   P->joins_bytes = a256b(sizeof(BJoin) * std::max(n, 1));
@@ -589,8 +647,9 @@ SJ_EXPORT sj_status sj_batch_plan_launch(sj_batch_plan* P, sj_stream_t stream) {
   if (P->dev.n_items == 0) return SJ_OK;
   const int grid = resident_ctas(P);
   KernelTimer timer("batch_persistent", s);
-  dispatch_kg(P->key_type, P->params.group_width, [&](auto k, auto g) {
-    batch_persistent_kernel<decltype(k), decltype(g)::value><<<grid, P->params.block_size, 0, s>>>(P->dev);
+  dispatch_kg(P->key_type, P->params.group_width, P->shape, [&](auto k, auto g, auto sh) {
+    batch_persistent_kernel<decltype(k), decltype(g)::value, decltype(sh)::value>
+        <<<grid, P->params.block_size, 0, s>>>(P->dev);
   });
   SJ_CUDA_TRY(cudaGetLastError());
   return SJ_OK;
@@ -634,11 +693,12 @@ SJ_EXPORT sj_status sj_batch_plan_launch_per_join(sj_batch_plan* P, sj_stream_t 
     const BJoin& J = P->host_joins[j];
     const int gb = std::max(1, std::min(J.build_tiles, cap));
     const int gp = std::max(1, std::min(P->probe_tiles[j], cap));
-    dispatch_kg(P->key_type, P->params.group_width, [&](auto k, auto g) {
+    dispatch_kg(P->key_type, P->params.group_width, P->shape, [&](auto k, auto g, auto sh) {
       using K = decltype(k);
       if (J.build_tiles > 0) batch_build_one_kernel<K><<<gb, block, 0, s>>>(P->dev, j);
       if (P->probe_tiles[j] > 0)
-        batch_probe_one_kernel<K, decltype(g)::value><<<gp, block, 0, s>>>(P->dev, j, P->probe_tiles[j]);
+        batch_probe_one_kernel<K, decltype(g)::value, decltype(sh)::value><<<gp, block, 0, s>>>(P->dev, j,
+                                                                                                P->probe_tiles[j]);
     });
   }
   SJ_CUDA_TRY(cudaGetLastError());

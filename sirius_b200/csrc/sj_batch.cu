@@ -274,16 +274,33 @@ __device__ void probe_tile_r(const BatchDev& P, const BJoin& J, int32_t join, in
   const int64_t hi = min(J.np, lo + P.tile_rows);
   const uint64_t mask = (1ull << J.log2_nb) - 1;
   const bool has_pp = SH || J.ppay.data != nullptr, has_bp = SH || J.bpay.data != nullptr;
-  for (int64_t base = lo + (int64_t)(threadIdx.x >> 5) * 32 * R; base < hi; base += (int64_t)nwarps * 32 * R) {
+  const int64_t stride = (int64_t)nwarps * 32 * R;
+  // the keys and probe payloads of the warp's next step load while this step probes
+  K kn[R];
+  uint64_t pn[R];
+  auto load_step = [&](int64_t sb) {
+#pragma unroll
+    for (int j = 0; j < R; ++j) {
+      const int64_t i = sb + 32 * j + lane;
+      kn[j] = i < hi ? load_key<K>(J.pkey, i) : (K)0;
+      pn[j] = i < hi && has_pp ? pay_load<SH>(J.ppay, i) : 0;
+    }
+  };
+  load_step(lo + (int64_t)(threadIdx.x >> 5) * 32 * R);
+  for (int64_t base = lo + (int64_t)(threadIdx.x >> 5) * 32 * R; base < hi; base += stride) {
     K k[R];
     uint64_t b[R], pv[R];
     uint32_t act = 0;
 #pragma unroll
     for (int j = 0; j < R; ++j) {
+      k[j] = kn[j];
+      pv[j] = pn[j];
+    }
+    if (base + stride < hi) load_step(base + stride);
+#pragma unroll
+    for (int j = 0; j < R; ++j) {
       const int64_t i = base + 32 * j + lane;
       const bool live = i < hi && bit_valid(J.pvalid, J.pvoff, i);
-      k[j] = live ? load_key<K>(J.pkey, i) : (K)0;
-      pv[j] = live && has_pp ? pay_load<SH>(J.ppay, i) : 0;  // in flight with the key
       b[j] = live ? bhome<K>(J, k[j]) : 0;
       if (live) act |= 1u << j;
     }

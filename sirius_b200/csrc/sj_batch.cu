@@ -244,8 +244,9 @@ __device__ void probe_tile(const BatchDev& P, const BJoin& J, int32_t join, int3
 }
 
 // Group width 1: each lane keeps kBatchR probe rows in flight (rows base + 32 j + lane, so every
-// key load is one coalesced warp access). Two rows per lane (3 CTAs of 256 per SM) beat one row
-// (4 CTAs) by 18 % and four rows (2 CTAs) by 36 % on 4,096 joins. A step probes one bucket for
+// key load is one coalesced warp access). On 4,096 joins with the staged write-out: two rows per
+// lane (4 CTAs of 256 per SM, 64 registers) 99.6 ms; one row (6 or 8 CTAs) 131.6 / 141.3 ms; three
+// rows (3 CTAs) 123.6 ms; four rows (2 CTAs) 139.2 ms. A step probes one bucket for
 // each of the lane's live rows. When every row has at most one match in the step (unique build
 // keys), all loads a match needs are in flight before the warp reserves its output range: the
 // probe payload loads with the key, the build payload (by row id) right after the bucket match;
@@ -264,11 +265,51 @@ __device__ __forceinline__ uint64_t pay_load(const PayloadIn& in, int64_t i) {
   else return load_elem(in.data, i, in.width);
 }
 
+// Staged write-out (compile-time shapes, SH = 4 or 8): all warps probing one join reserve output on
+// the join's one counter, and with one atomicAdd per 64-row step that address serialises the
+// launch (spreading it over 32 counters, in a timing-only copy, took the 4,096-join sweep from 120
+// to 99 ms). So a warp collects its matches in a shared-memory area of kStage rows (probe row id,
+// build row id, both payloads) and reserves output once per ~kStage - 64 matches, then writes the
+// area out in contiguous runs. No holes: a flush reserves exactly the rows it holds.
+constexpr int kStage = 256;
+
+template <int SH>
+constexpr int stage_row_bytes() { return 8 + 2 * SH; }
+
+// dynamic shared memory of a CTA of `block` threads for output shape `sh`
+static inline size_t stage_smem(int sh, int block) {
+  return sh ? (size_t)(block / 32) * kStage * (size_t)(8 + 2 * sh) : 0;
+}
+
 template <typename K, int SH>
 __device__ void probe_tile_r(const BatchDev& P, const BJoin& J, int32_t join, int32_t tile) {
   constexpr int S = BTable<K>::kSlots;
   constexpr int R = kBatchR;
   const int lane = threadIdx.x & 31;
+  // this warp's staging area: prid[kStage] | brid[kStage] | probe payload[kStage] | build payload[kStage]
+  extern __shared__ __align__(16) unsigned char s_stage[];
+  using PW = std::conditional_t<SH == 8, unsigned long long, unsigned int>;
+  int32_t* st_prid = reinterpret_cast<int32_t*>(s_stage + (size_t)(threadIdx.x >> 5) * kStage * stage_row_bytes<SH>());
+  int32_t* st_brid = st_prid + kStage;
+  PW* st_pp = reinterpret_cast<PW*>(st_brid + kStage);
+  PW* st_bp = st_pp + kStage;
+  uint32_t fill = 0;  // rows staged (warp-uniform)
+  auto flush = [&]() {
+    __syncwarp();
+    unsigned long long pos = 0;
+    if (lane == 0) pos = atomicAdd(P.counts + join, (unsigned long long)fill);
+    pos = __shfl_sync(kFullMask, pos, 0);
+    for (uint32_t e = lane; e < fill; e += 32) {
+      const int64_t p = (int64_t)(pos + e);
+      if (p >= J.capacity) break;
+      __stcs(J.out_prid + p, st_prid[e]);
+      __stcs(J.out_brid + p, st_brid[e]);
+      __stcs(static_cast<PW*>(J.out_ppay.data) + p, st_pp[e]);
+      __stcs(static_cast<PW*>(J.out_bpay.data) + p, st_bp[e]);
+    }
+    __syncwarp();
+    fill = 0;
+  };
   const int nwarps = blockDim.x >> 5;
   const int64_t lo = (int64_t)tile * P.tile_rows;
   const int64_t hi = min(J.np, lo + P.tile_rows);
@@ -363,14 +404,30 @@ __device__ void probe_tile_r(const BatchDev& P, const BJoin& J, int32_t join, in
           tot += __popc(bal[j]);
         }
         if (tot == 0) continue;
-        unsigned long long pos = 0;
-        if (lane == 0) pos = atomicAdd(P.counts + join, (unsigned long long)tot);
-        pos = __shfl_sync(kFullMask, pos, 0);
         const unsigned below = (1u << lane) - 1u;
+        if constexpr (SH != 0) {
+          uint32_t run = fill;
 #pragma unroll
-        for (int j = 0; j < R; ++j) {
-          if (m[j]) put((int64_t)(pos + __popc(bal[j] & below)), base + 32 * j + lane, brow[j], pv[j], bv[j]);
-          pos += __popc(bal[j]);
+          for (int j = 0; j < R; ++j) {
+            const uint32_t e = run + __popc(bal[j] & below);
+            run += __popc(bal[j]);
+            if (!m[j]) continue;
+            st_prid[e] = (int32_t)(base + 32 * j + lane);
+            st_brid[e] = brow[j];
+            st_pp[e] = (PW)pv[j];
+            st_bp[e] = (PW)bv[j];
+          }
+          fill = run;
+          if (fill > (uint32_t)(kStage - 32 * R)) flush();  // the next step could not fit
+        } else {
+          unsigned long long pos = 0;
+          if (lane == 0) pos = atomicAdd(P.counts + join, (unsigned long long)tot);
+          pos = __shfl_sync(kFullMask, pos, 0);
+#pragma unroll
+          for (int j = 0; j < R; ++j) {
+            if (m[j]) put((int64_t)(pos + __popc(bal[j] & below)), base + 32 * j + lane, brow[j], pv[j], bv[j]);
+            pos += __popc(bal[j]);
+          }
         }
       } else {
         // duplicates in one bucket: lane-major positions
@@ -385,6 +442,9 @@ __device__ void probe_tile_r(const BatchDev& P, const BJoin& J, int32_t join, in
                   has_bp ? pay_load<SH>(J.bpay, rid[j][q]) : 0);
       }
     }
+  }
+  if constexpr (SH != 0) {
+    if (fill) flush();
   }
 }
 
@@ -524,9 +584,10 @@ static int resident_ctas(sj_batch_plan* P) {
   int per_sm = 0;
   const int block = P->params.block_size;
   dispatch_kg(P->key_type, P->params.group_width, P->shape, [&](auto k, auto g, auto sh) {
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm,
-                                                  batch_persistent_kernel<decltype(k), decltype(g)::value, decltype(sh)::value>,
-                                                  block, 0);
+    auto* kern = batch_persistent_kernel<decltype(k), decltype(g)::value, decltype(sh)::value>;
+    const size_t smem = stage_smem(decltype(g)::value == 1 ? decltype(sh)::value : 0, block);
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, block, smem);
   });
   per_sm = std::max(1, std::min(per_sm, P->params.ctas_per_sm));
   return per_sm * sm_count(P->device);
@@ -665,8 +726,9 @@ SJ_EXPORT sj_status sj_batch_plan_launch(sj_batch_plan* P, sj_stream_t stream) {
   const int grid = resident_ctas(P);
   KernelTimer timer("batch_persistent", s);
   dispatch_kg(P->key_type, P->params.group_width, P->shape, [&](auto k, auto g, auto sh) {
+    const size_t smem = stage_smem(decltype(g)::value == 1 ? decltype(sh)::value : 0, P->params.block_size);
     batch_persistent_kernel<decltype(k), decltype(g)::value, decltype(sh)::value>
-        <<<grid, P->params.block_size, 0, s>>>(P->dev);
+        <<<grid, P->params.block_size, smem, s>>>(P->dev);
   });
   SJ_CUDA_TRY(cudaGetLastError());
   return SJ_OK;
@@ -705,6 +767,11 @@ SJ_EXPORT sj_status sj_batch_plan_launch_per_join(sj_batch_plan* P, sj_stream_t 
   SJ_TRY(reset_batch(P, s));
   const int block = P->params.block_size;
   const int cap = sm_count(P->device) * P->params.ctas_per_sm;
+  dispatch_kg(P->key_type, P->params.group_width, P->shape, [&](auto k, auto g, auto sh) {
+    const size_t smem = stage_smem(decltype(g)::value == 1 ? decltype(sh)::value : 0, block);
+    cudaFuncSetAttribute(batch_probe_one_kernel<decltype(k), decltype(g)::value, decltype(sh)::value>,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  });
   KernelTimer timer("batch_per_join", s);
   for (int32_t j = 0; j < P->n_joins; ++j) {
     const BJoin& J = P->host_joins[j];
@@ -713,9 +780,11 @@ SJ_EXPORT sj_status sj_batch_plan_launch_per_join(sj_batch_plan* P, sj_stream_t 
     dispatch_kg(P->key_type, P->params.group_width, P->shape, [&](auto k, auto g, auto sh) {
       using K = decltype(k);
       if (J.build_tiles > 0) batch_build_one_kernel<K><<<gb, block, 0, s>>>(P->dev, j);
-      if (P->probe_tiles[j] > 0)
-        batch_probe_one_kernel<K, decltype(g)::value, decltype(sh)::value><<<gp, block, 0, s>>>(P->dev, j,
-                                                                                                P->probe_tiles[j]);
+      if (P->probe_tiles[j] > 0) {
+        auto* kern = batch_probe_one_kernel<K, decltype(g)::value, decltype(sh)::value>;
+        const size_t smem = stage_smem(decltype(g)::value == 1 ? decltype(sh)::value : 0, block);
+        kern<<<gp, block, smem, s>>>(P->dev, j, P->probe_tiles[j]);
+      }
     });
   }
   SJ_CUDA_TRY(cudaGetLastError());

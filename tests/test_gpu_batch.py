@@ -12,18 +12,18 @@ from sirius_b200 import batch as B
 pytestmark = pytest.mark.gpu
 
 
-def _specs(dev, seed, n_joins, dtype, dup=True, nulls=True):
+def _specs(dev, seed, n_joins, dtype, dup=True, nulls=True, pay=(np.int32, np.int64), max_build=6000):
     rng = np.random.default_rng(seed)
     host, specs = [], []
     for j in range(n_joins):
-        nb = int(np.exp(rng.uniform(np.log(1), np.log(6000))))
+        nb = int(np.exp(rng.uniform(np.log(1), np.log(max_build))))
         npr = int(rng.integers(0, 4 * nb + 3))
         bk = (rng.integers(0, max(1, nb // 2), nb) if (dup and j % 3 == 0) else rng.permutation(nb)).astype(dtype)
         pk = rng.integers(-2, int(1.3 * nb) + 2, npr).astype(dtype)
         bv = O.pack_validity(rng.random(nb) > 0.1) if (nulls and j % 4 == 1) else None
         pv = O.pack_validity(rng.random(npr) > 0.1) if (nulls and j % 5 == 2) else None
-        bp = rng.integers(0, 1 << 30, nb).astype(np.int32)
-        pp = rng.integers(0, 1 << 40, npr).astype(np.int64)
+        bp = rng.integers(0, 1 << 30, nb).astype(pay[0])
+        pp = rng.integers(0, 1 << 40, npr).astype(pay[1])
         cnt = O.hash_join_count(bk, pk, bv, pv)
         host.append((bk, pk, bv, pv, bp, pp, cnt))
         specs.append(B.BatchJoinSpec(dev_t(bk, dev), dev_t(pk, dev), dev_t(bp, dev), dev_t(pp, dev),
@@ -84,3 +84,66 @@ def test_batch_empty_joins(cuda):
         counts, err = plan.counts()
         torch.cuda.synchronize()
         assert counts.tolist() == [0, 0, 100] and int(err.item()) == 0
+
+
+@pytest.mark.parametrize("width", [4, 8])
+@pytest.mark.parametrize("dtype", [np.int32, np.int64])
+@pytest.mark.parametrize("block", [128, 256, 512])
+def test_batch_staged_output_shapes(cuda, width, dtype, block):
+    """Both payloads of one width (4 or 8 bytes, no payload NULLs) and both row ids: the compile-time
+    shape whose warps stage matches in shared memory and reserve output once per flush. Joins up to
+    60K build rows (several flushes per warp), duplicates and NULL keys mixed in."""
+    t = np.int32 if width == 4 else np.int64
+    host, specs = _specs(cuda, 31 + width + block, 40, dtype, pay=(t, t), max_build=60_000)
+    s = torch.cuda.Stream()
+    with B.BatchPlan(specs, B.batch_params(block_size=block, tile_rows=4096), stream=s) as plan:
+        plan.launch(s)
+        s.synchronize()
+        _check(host, plan)
+        for _ in range(2):
+            plan.replay(s)
+        s.synchronize()
+        _check(host, plan)
+        plan.launch_per_join(s)
+        s.synchronize()
+        _check(host, plan)
+
+
+SENTINEL, GUARD = -7, 512
+
+
+def test_batch_staged_capacity_below_count(cuda):
+    """Capacities below the match count: every count is still reported in full, nothing is written
+    past a join's capacity, and the rows written are real matches."""
+    rng = np.random.default_rng(77)
+    host, specs = [], []
+    for j in range(24):
+        nb = int(rng.integers(1000, 40_000))
+        bk = rng.permutation(nb).astype(np.int32)
+        pk = rng.integers(0, nb, 8 * nb).astype(np.int32)   # every probe row matches
+        bp = rng.integers(0, 1 << 30, nb).astype(np.int32)
+        pp = rng.integers(0, 1 << 30, len(pk)).astype(np.int32)
+        cap = int(len(pk) * rng.uniform(0.1, 0.95))
+        # outputs with GUARD rows past the capacity, which must keep their SENTINEL
+        out = B.BatchJoinOutput(*[torch.full((cap + GUARD,), SENTINEL, dtype=torch.int32, device=cuda)
+                                  for _ in range(4)])
+        sp = B.BatchJoinSpec(dev_t(bk, cuda), dev_t(pk, cuda), dev_t(bp, cuda), dev_t(pp, cuda), capacity=cap,
+                             out=out)
+        host.append((bk, pk, bp, pp, cap))
+        specs.append(sp)
+    with B.BatchPlan(specs, B.batch_params(tile_rows=4096)) as plan:
+        plan.launch()
+        counts, err = plan.counts()
+        torch.cuda.synchronize()
+        assert int(err.item()) == 0
+        for (bk, pk, bp, pp, cap), s, c in zip(host, plan.specs, counts.cpu().numpy()):
+            assert c == len(pk)
+            cols = [x.cpu().numpy() for x in (s.out.probe_rid, s.out.build_rid, s.out.probe_payload,
+                                              s.out.build_payload)]
+            for x in cols:
+                assert (x[cap:] == SENTINEL).all(), "a row was written past the capacity"
+            prid, brid, ppo, bpo = [x[:cap] for x in cols]
+            assert np.array_equal(pk[prid], bk[brid])
+            assert np.array_equal(ppo, pp[prid])
+            assert np.array_equal(bpo, bp[brid])
+            assert len(np.unique(prid)) == cap   # distinct probe rows, no row written twice

@@ -246,14 +246,17 @@ __device__ void probe_tile(const BatchDev& P, const BJoin& J, int32_t join, int3
 // Group width 1: each lane keeps kBatchR probe rows in flight (rows base + 32 j + lane, so every
 // key load is one coalesced warp access). On 4,096 joins with the staged write-out: two rows per
 // lane (4 CTAs of 256 per SM, 64 registers) 99.6 ms; one row (6 or 8 CTAs) 131.6 / 141.3 ms; three
-// rows (3 CTAs) 123.6 ms; four rows (2 CTAs) 139.2 ms. A step probes one bucket for
-// each of the lane's live rows. When every row has at most one match in the step (unique build
-// keys), all loads a match needs are in flight before the warp reserves its output range: the
-// probe payload loads with the key, the build payload (by row id) right after the bucket match;
-// group j's hit lanes are then ranked with a ballot so each output column is written as one
-// contiguous run per group. Otherwise (duplicates in one bucket) positions follow (lane, row
-// group, slot) order. A row stops at its first bucket with an EMPTY slot (its matches there still
-// count) or once the whole table has been scanned.
+// rows (3 CTAs) 123.6 ms; four rows (2 CTAs) 139.2 ms.
+// A step probes each row's home bucket. A row stops at its first bucket with an EMPTY slot (its
+// matches there still count) or once the whole table has been scanned. The few rows whose home
+// bucket is full (about 7 % at load factor 0.35) go to a per-warp list in shared memory with their
+// next bucket, and the warp probes that list 32 rows at a time, with every lane busy, whenever it
+// holds 32 rows, and at the end of the tile. Walking them in the step instead cost the whole warp
+// one more pass over the step's code for a handful of lanes, in almost every step.
+// When every row has at most one match in a pass (unique build keys), all loads a match needs are
+// in flight before the warp reserves output: the probe payload loads with the key, the build
+// payload (by row id) right after the bucket match; hit lanes are ranked with ballots. Otherwise
+// (duplicates in one bucket) positions follow (lane, row, slot) order.
 constexpr int kBatchR = 2;
 
 // SH = 4 or 8: every join of the plan gathers one probe and one build payload of SH bytes without
@@ -272,13 +275,16 @@ __device__ __forceinline__ uint64_t pay_load(const PayloadIn& in, int64_t i) {
 // build row id, both payloads) and reserves output once per ~kStage - 64 matches, then writes the
 // area out in contiguous runs. No holes: a flush reserves exactly the rows it holds.
 constexpr int kStage = 256;
+// per-warp list of rows that go on to their next bucket: {probe row, bucket}; it holds fewer than
+// 32 rows between passes, plus at most 32 * kBatchR added by one step
+constexpr int kMore = 128;
 
 template <int SH>
 constexpr int stage_row_bytes() { return 8 + 2 * SH; }
 
-// dynamic shared memory of a CTA of `block` threads for output shape `sh`
+// dynamic shared memory of a CTA of `block` threads for output shape `sh` (group width 1)
 static inline size_t stage_smem(int sh, int block) {
-  return sh ? (size_t)(block / 32) * kStage * (size_t)(8 + 2 * sh) : 0;
+  return (size_t)(block / 32) * ((sh ? (size_t)kStage * (8 + 2 * sh) : 0) + (size_t)kMore * 8);
 }
 
 template <typename K, int SH>
@@ -286,14 +292,27 @@ __device__ void probe_tile_r(const BatchDev& P, const BJoin& J, int32_t join, in
   constexpr int S = BTable<K>::kSlots;
   constexpr int R = kBatchR;
   const int lane = threadIdx.x & 31;
-  // this warp's staging area: prid[kStage] | brid[kStage] | probe payload[kStage] | build payload[kStage]
-  extern __shared__ __align__(16) unsigned char s_stage[];
+  const unsigned below = (1u << lane) - 1u;
+  const int nwarps = blockDim.x >> 5;
+  const int64_t lo = (int64_t)tile * P.tile_rows;
+  const int64_t hi = min(J.np, lo + P.tile_rows);
+  const uint64_t mask = (1ull << J.log2_nb) - 1;
+  const bool has_pp = SH || J.ppay.data != nullptr, has_bp = SH || J.bpay.data != nullptr;
+  const int64_t stride = (int64_t)nwarps * 32 * R;
+  // this warp's shared memory: [prid | brid | probe payload | build payload] x kStage (SH != 0),
+  // then the list of rows that continue: row[kMore] | bucket[kMore]
+  extern __shared__ __align__(16) unsigned char s_dyn[];
   using PW = std::conditional_t<SH == 8, unsigned long long, unsigned int>;
-  int32_t* st_prid = reinterpret_cast<int32_t*>(s_stage + (size_t)(threadIdx.x >> 5) * kStage * stage_row_bytes<SH>());
+  unsigned char* wbase = s_dyn + (size_t)(threadIdx.x >> 5) * ((SH ? (size_t)kStage * stage_row_bytes<SH>() : 0) +
+                                                               (size_t)kMore * 8);
+  int32_t* st_prid = reinterpret_cast<int32_t*>(wbase);
   int32_t* st_brid = st_prid + kStage;
   PW* st_pp = reinterpret_cast<PW*>(st_brid + kStage);
   PW* st_bp = st_pp + kStage;
+  int32_t* more_row = reinterpret_cast<int32_t*>(wbase + (SH ? (size_t)kStage * stage_row_bytes<SH>() : 0));
+  uint32_t* more_b = reinterpret_cast<uint32_t*>(more_row + kMore);
   uint32_t fill = 0;  // rows staged (warp-uniform)
+  uint32_t n_more = 0;  // rows in the continue list (warp-uniform)
   auto flush = [&]() {
     __syncwarp();
     unsigned long long pos = 0;
@@ -310,12 +329,129 @@ __device__ void probe_tile_r(const BatchDev& P, const BJoin& J, int32_t join, in
     __syncwarp();
     fill = 0;
   };
-  const int nwarps = blockDim.x >> 5;
-  const int64_t lo = (int64_t)tile * P.tile_rows;
-  const int64_t hi = min(J.np, lo + P.tile_rows);
-  const uint64_t mask = (1ull << J.log2_nb) - 1;
-  const bool has_pp = SH || J.ppay.data != nullptr, has_bp = SH || J.bpay.data != nullptr;
-  const int64_t stride = (int64_t)nwarps * 32 * R;
+  // write one match: output position p, probe row i, build row id brow, payloads
+  auto put = [&](int64_t p, int64_t i, int32_t brow, uint64_t pval, uint64_t bval) {
+    if (p >= J.capacity) return;
+    if constexpr (SH != 0) {
+      __stcs(J.out_prid + p, (int32_t)i);
+      __stcs(J.out_brid + p, brow);
+      __stcs(static_cast<PW*>(J.out_ppay.data) + p, (PW)pval);
+      __stcs(static_cast<PW*>(J.out_bpay.data) + p, (PW)bval);
+      return;
+    }
+    if (J.out_prid) J.out_prid[p] = (int32_t)i;
+    if (J.out_brid) J.out_brid[p] = brow;
+    if (has_pp) {
+      store_elem(J.out_ppay.data, p, J.ppay.width, pval);
+      if (J.ppay.valid && bit_valid(J.ppay.valid, J.ppay.voff, i)) set_out_bit(J.out_ppay.valid, p);
+    }
+    if (has_bp) {
+      store_elem(J.out_bpay.data, p, J.bpay.width, bval);
+      if (J.bpay.valid && bit_valid(J.bpay.valid, J.bpay.voff, brow)) set_out_bit(J.out_bpay.valid, p);
+    }
+  };
+  // the matches m[j] (slot bits, row ids rid[j]) of probe rows row[j], j < NR, with probe payloads pv
+  auto emit = [&](const uint32_t (&m)[R], const int32_t (&rid)[R][4], const int64_t (&row)[R],
+                  const uint64_t (&pv)[R]) {
+    bool single = true;  // at most one match per row (always so for unique builds)
+#pragma unroll
+    for (int j = 0; j < R; ++j) single &= (m[j] & (m[j] - 1u)) == 0;
+    if (__all_sync(kFullMask, single)) {
+      int32_t brow[R];
+      uint64_t bv[R];
+      unsigned bal[R];
+      uint32_t tot = 0;
+#pragma unroll
+      for (int j = 0; j < R; ++j) {
+        brow[j] = 0;
+#pragma unroll
+        for (int q = 0; q < S; ++q) brow[j] = (m[j] >> q & 1u) ? rid[j][q] : brow[j];
+        bv[j] = m[j] && has_bp ? pay_load<SH>(J.bpay, brow[j]) : 0;
+        bal[j] = __ballot_sync(kFullMask, m[j] != 0);
+        tot += __popc(bal[j]);
+      }
+      if (tot == 0) return;
+      if constexpr (SH != 0) {
+        if (fill + tot > (uint32_t)kStage) flush();
+        uint32_t run = fill;
+#pragma unroll
+        for (int j = 0; j < R; ++j) {
+          const uint32_t e = run + __popc(bal[j] & below);
+          run += __popc(bal[j]);
+          if (!m[j]) continue;
+          st_prid[e] = (int32_t)row[j];
+          st_brid[e] = brow[j];
+          st_pp[e] = (PW)pv[j];
+          st_bp[e] = (PW)bv[j];
+        }
+        fill = run;
+        if (fill > (uint32_t)(kStage - 32 * R)) flush();  // the next pass could not fit
+      } else {
+        unsigned long long pos = 0;
+        if (lane == 0) pos = atomicAdd(P.counts + join, (unsigned long long)tot);
+        pos = __shfl_sync(kFullMask, pos, 0);
+#pragma unroll
+        for (int j = 0; j < R; ++j) {
+          if (m[j]) put((int64_t)(pos + __popc(bal[j] & below)), row[j], brow[j], pv[j], bv[j]);
+          pos += __popc(bal[j]);
+        }
+      }
+    } else {
+      // duplicates in one bucket: lane-major positions
+      uint32_t cnt = 0;
+#pragma unroll
+      for (int j = 0; j < R; ++j) cnt += __popc(m[j]);
+      const unsigned long long pos0 = warp_reserve(P.counts + join, cnt);
+      uint32_t r = 0;
+#pragma unroll
+      for (int j = 0; j < R; ++j)
+#pragma unroll
+        for (int q = 0; q < S; ++q)
+          if (m[j] >> q & 1u)
+            put((int64_t)pos0 + r++, row[j], rid[j][q], pv[j], has_bp ? pay_load<SH>(J.bpay, rid[j][q]) : 0);
+    }
+  };
+  // rows whose bucket had no EMPTY slot (cont[j]) join the list with their next bucket
+  auto keep_on = [&](const bool (&cont)[R], const int64_t (&row)[R], const uint64_t (&b)[R]) {
+#pragma unroll
+    for (int j = 0; j < R; ++j) {
+      const unsigned bal = __ballot_sync(kFullMask, cont[j]);
+      if (cont[j]) {
+        const uint32_t e = n_more + __popc(bal & below);
+        more_row[e] = (int32_t)row[j];
+        more_b[e] = (uint32_t)((b[j] + 1) & mask);
+      }
+      n_more += __popc(bal);
+    }
+    __syncwarp();
+  };
+  // one pass over the last `take` (<= 32) rows of the list, one row per lane
+  auto walk_more = [&](uint32_t take) {
+    const bool mine = (uint32_t)lane < take;
+    int64_t row[R] = {};
+    uint64_t b[R] = {}, pv[R] = {};
+    uint32_t m[R] = {};
+    int32_t rid[R][4] = {};
+    bool cont[R] = {};
+    if (mine) {
+      row[0] = more_row[n_more - take + lane];
+      b[0] = more_b[n_more - take + lane];
+    }
+    __syncwarp();
+    n_more -= take;
+    if (mine) {
+      const K k = load_key<K>(J.pkey, row[0]);
+      pv[0] = has_pp ? pay_load<SH>(J.ppay, row[0]) : 0;
+      bool has_empty = false;
+      m[0] = BTable<K>::probe(P.arena, J.bucket_off + b[0], k, has_empty, rid[0]);
+      // buckets probed before this one: (b - home) mod the table size; the whole table is scanned
+      // once it reaches the last bucket
+      const uint64_t before = (b[0] - bhome<K>(J, k)) & mask;
+      cont[0] = !has_empty && before < mask;
+    }
+    emit(m, rid, row, pv);
+    keep_on(cont, row, b);
+  };
   // the keys and probe payloads of the warp's next step load while this step probes
   K kn[R];
   uint64_t pn[R];
@@ -331,118 +467,33 @@ __device__ void probe_tile_r(const BatchDev& P, const BJoin& J, int32_t join, in
   for (int64_t base = lo + (int64_t)(threadIdx.x >> 5) * 32 * R; base < hi; base += stride) {
     K k[R];
     uint64_t b[R], pv[R];
-    uint32_t act = 0;
+    int64_t row[R];
 #pragma unroll
     for (int j = 0; j < R; ++j) {
       k[j] = kn[j];
       pv[j] = pn[j];
     }
     if (base + stride < hi) load_step(base + stride);
+    uint32_t m[R];
+    int32_t rid[R][4];
+    bool cont[R];
 #pragma unroll
     for (int j = 0; j < R; ++j) {
-      const int64_t i = base + 32 * j + lane;
-      const bool live = i < hi && bit_valid(J.pvalid, J.pvoff, i);
+      row[j] = base + 32 * j + lane;
+      const bool live = row[j] < hi && bit_valid(J.pvalid, J.pvoff, row[j]);
       b[j] = live ? bhome<K>(J, k[j]) : 0;
-      if (live) act |= 1u << j;
+      m[j] = 0;
+      cont[j] = false;
+      if (!live) continue;
+      bool has_empty = false;
+      m[j] = BTable<K>::probe(P.arena, J.bucket_off + b[j], k[j], has_empty, rid[j]);
+      cont[j] = !has_empty && mask > 0;
     }
-    for (uint64_t step = 0; __any_sync(kFullMask, act != 0); ++step) {
-      uint32_t m[R];
-      int32_t rid[R][4];
-      uint32_t cnt = 0;
-#pragma unroll
-      for (int j = 0; j < R; ++j) {
-        m[j] = 0;
-        if (!(act >> j & 1u)) continue;
-        bool has_empty = false;
-        m[j] = BTable<K>::probe(P.arena, J.bucket_off + b[j], k[j], has_empty, rid[j]);
-        cnt += __popc(m[j]);
-        if (has_empty || step >= mask) act &= ~(1u << j);
-        else b[j] = (b[j] + 1) & mask;
-      }
-      // write one match: output position p, probe row i, build row id brow, payloads
-      auto put = [&](int64_t p, int64_t i, int32_t brow, uint64_t pval, uint64_t bval) {
-        if (p >= J.capacity) return;
-        if constexpr (SH != 0) {
-          __stcs(J.out_prid + p, (int32_t)i);
-          __stcs(J.out_brid + p, brow);
-          if constexpr (SH == 8) {
-            __stcs(static_cast<unsigned long long*>(J.out_ppay.data) + p, (unsigned long long)pval);
-            __stcs(static_cast<unsigned long long*>(J.out_bpay.data) + p, (unsigned long long)bval);
-          } else {
-            __stcs(static_cast<unsigned int*>(J.out_ppay.data) + p, (unsigned int)pval);
-            __stcs(static_cast<unsigned int*>(J.out_bpay.data) + p, (unsigned int)bval);
-          }
-          return;
-        }
-        if (J.out_prid) J.out_prid[p] = (int32_t)i;
-        if (J.out_brid) J.out_brid[p] = brow;
-        if (has_pp) {
-          store_elem(J.out_ppay.data, p, J.ppay.width, pval);
-          if (J.ppay.valid && bit_valid(J.ppay.valid, J.ppay.voff, i)) set_out_bit(J.out_ppay.valid, p);
-        }
-        if (has_bp) {
-          store_elem(J.out_bpay.data, p, J.bpay.width, bval);
-          if (J.bpay.valid && bit_valid(J.bpay.valid, J.bpay.voff, brow)) set_out_bit(J.out_bpay.valid, p);
-        }
-      };
-      bool single = true;  // at most one match per row in this step (always so for unique builds)
-#pragma unroll
-      for (int j = 0; j < R; ++j) single &= (m[j] & (m[j] - 1u)) == 0;
-      if (__all_sync(kFullMask, single)) {
-        // the matched build rows and their payloads first, then one reservation per warp
-        int32_t brow[R];
-        uint64_t bv[R];
-        unsigned bal[R];
-        uint32_t tot = 0;
-#pragma unroll
-        for (int j = 0; j < R; ++j) {
-          brow[j] = 0;
-#pragma unroll
-          for (int q = 0; q < S; ++q) brow[j] = (m[j] >> q & 1u) ? rid[j][q] : brow[j];
-          bv[j] = m[j] && has_bp ? pay_load<SH>(J.bpay, brow[j]) : 0;
-          bal[j] = __ballot_sync(kFullMask, m[j] != 0);
-          tot += __popc(bal[j]);
-        }
-        if (tot == 0) continue;
-        const unsigned below = (1u << lane) - 1u;
-        if constexpr (SH != 0) {
-          uint32_t run = fill;
-#pragma unroll
-          for (int j = 0; j < R; ++j) {
-            const uint32_t e = run + __popc(bal[j] & below);
-            run += __popc(bal[j]);
-            if (!m[j]) continue;
-            st_prid[e] = (int32_t)(base + 32 * j + lane);
-            st_brid[e] = brow[j];
-            st_pp[e] = (PW)pv[j];
-            st_bp[e] = (PW)bv[j];
-          }
-          fill = run;
-          if (fill > (uint32_t)(kStage - 32 * R)) flush();  // the next step could not fit
-        } else {
-          unsigned long long pos = 0;
-          if (lane == 0) pos = atomicAdd(P.counts + join, (unsigned long long)tot);
-          pos = __shfl_sync(kFullMask, pos, 0);
-#pragma unroll
-          for (int j = 0; j < R; ++j) {
-            if (m[j]) put((int64_t)(pos + __popc(bal[j] & below)), base + 32 * j + lane, brow[j], pv[j], bv[j]);
-            pos += __popc(bal[j]);
-          }
-        }
-      } else {
-        // duplicates in one bucket: lane-major positions
-        const unsigned long long pos0 = warp_reserve(P.counts + join, cnt);
-        uint32_t r = 0;
-#pragma unroll
-        for (int j = 0; j < R; ++j)
-#pragma unroll
-          for (int q = 0; q < S; ++q)
-            if (m[j] >> q & 1u)
-              put((int64_t)pos0 + r++, base + 32 * j + lane, rid[j][q], pv[j],
-                  has_bp ? pay_load<SH>(J.bpay, rid[j][q]) : 0);
-      }
-    }
+    emit(m, rid, row, pv);
+    keep_on(cont, row, b);
+    while (n_more >= 32) walk_more(32);
   }
+  while (n_more > 0) walk_more(n_more < 32 ? n_more : 32);
   if constexpr (SH != 0) {
     if (fill) flush();
   }
@@ -585,7 +636,7 @@ static int resident_ctas(sj_batch_plan* P) {
   const int block = P->params.block_size;
   dispatch_kg(P->key_type, P->params.group_width, P->shape, [&](auto k, auto g, auto sh) {
     auto* kern = batch_persistent_kernel<decltype(k), decltype(g)::value, decltype(sh)::value>;
-    const size_t smem = stage_smem(decltype(g)::value == 1 ? decltype(sh)::value : 0, block);
+    const size_t smem = (decltype(g)::value == 1 ? stage_smem(decltype(sh)::value, block) : 0);
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, block, smem);
   });
@@ -726,7 +777,7 @@ SJ_EXPORT sj_status sj_batch_plan_launch(sj_batch_plan* P, sj_stream_t stream) {
   const int grid = resident_ctas(P);
   KernelTimer timer("batch_persistent", s);
   dispatch_kg(P->key_type, P->params.group_width, P->shape, [&](auto k, auto g, auto sh) {
-    const size_t smem = stage_smem(decltype(g)::value == 1 ? decltype(sh)::value : 0, P->params.block_size);
+    const size_t smem = (decltype(g)::value == 1 ? stage_smem(decltype(sh)::value, P->params.block_size) : 0);
     batch_persistent_kernel<decltype(k), decltype(g)::value, decltype(sh)::value>
         <<<grid, P->params.block_size, smem, s>>>(P->dev);
   });
@@ -768,7 +819,7 @@ SJ_EXPORT sj_status sj_batch_plan_launch_per_join(sj_batch_plan* P, sj_stream_t 
   const int block = P->params.block_size;
   const int cap = sm_count(P->device) * P->params.ctas_per_sm;
   dispatch_kg(P->key_type, P->params.group_width, P->shape, [&](auto k, auto g, auto sh) {
-    const size_t smem = stage_smem(decltype(g)::value == 1 ? decltype(sh)::value : 0, block);
+    const size_t smem = (decltype(g)::value == 1 ? stage_smem(decltype(sh)::value, block) : 0);
     cudaFuncSetAttribute(batch_probe_one_kernel<decltype(k), decltype(g)::value, decltype(sh)::value>,
                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   });
@@ -782,7 +833,7 @@ SJ_EXPORT sj_status sj_batch_plan_launch_per_join(sj_batch_plan* P, sj_stream_t 
       if (J.build_tiles > 0) batch_build_one_kernel<K><<<gb, block, 0, s>>>(P->dev, j);
       if (P->probe_tiles[j] > 0) {
         auto* kern = batch_probe_one_kernel<K, decltype(g)::value, decltype(sh)::value>;
-        const size_t smem = stage_smem(decltype(g)::value == 1 ? decltype(sh)::value : 0, block);
+        const size_t smem = (decltype(g)::value == 1 ? stage_smem(decltype(sh)::value, block) : 0);
         kern<<<gp, block, smem, s>>>(P->dev, j, P->probe_tiles[j]);
       }
     });

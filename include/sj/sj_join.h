@@ -164,7 +164,10 @@ typedef struct sj_join_params {
   int32_t null_equality;    /* sj_null_equality */
   float load_factor;        /* slots in use / slots; default 0.5 (the distinct_hash_join value) */
   int32_t block_size;       /* threads per CTA for probe kernels; default 256 */
-  int32_t group_width;      /* probe group width 1,2,4,8,16,32 lanes per key; default 1 */
+  int32_t group_width;      /* accepted and ignored: a single join's probe uses one lane per key,
+                               which loads a whole 32-byte bucket (4 or 2 slots) at once. Lanes
+                               sharing one key are the batched path's sj_batch_params.group_width,
+                               where one lane per key measured fastest. Default 1 */
   int32_t partition_bits;   /* radix bits of the partitioned variant: 0 = automatic (partition
                                when the table and its attached payloads outgrow L2), -1 = never,
                                1..10 = that many bits (2^bits partitions) */

@@ -313,6 +313,10 @@ def run_sj(args):
     with ClockSampler(dev.index) as clk:
         t_all0 = torch.cuda.Event(enable_timing=True)
         t_all1 = torch.cuda.Event(enable_timing=True)
+        # a ~2 ms spin kernel ahead of the start event, so the host has queued the first steps
+        # before the timed region starts: otherwise the first step also measures the host's
+        # first enqueue after the synchronize above (one step of 20 was seen at 3.1 ms vs 1.81)
+        torch.cuda._sleep(4_000_000)
         t_all0.record()
         for i in range(args.steps):
             starts[i].record()
@@ -415,6 +419,8 @@ def run_sj(args):
                        "probe_rows": args.n_probe, "parallelism": f"replicated build, probe sharded x{world}",
                        "l2": "no flush: every step streams 1 GiB of probe input and writes 2 GiB of output, "
                              "both larger than the 126 MB L2",
+                       "start": "a ~2 ms GPU spin kernel precedes the start event, so the host's enqueue of "
+                                "the first steps is not inside the timed region",
                        "table": {"layout": "DISTINCT" if info.layout == 1 else "GROUPED",
                                  "slot": "PACKED64" if info.slot_kind == 0 else "WIDE128",
                                  "slots": int(info.num_slots), "rid_bits": int(info.rid_bits),
@@ -426,6 +432,9 @@ def run_sj(args):
                          "unit_of_work": "probe phase = one sj_probe_gather call over 64M probe rows "
                                          "(partition + probe/gather kernels)",
                          "alg_bytes_per_launch": int(alg), "launch_ms": round(launch_ms, 4),
+                         "launch_ms_min_median_max": [round(min(per_launch), 4),
+                                                      round(statistics.median(per_launch), 4),
+                                                      round(max(per_launch), 4)],
                          "dominant_kernel": dominant, "kernels": kernels, "peak_source": peak_src,
                          "frac_of_nominal_8TBs": round(achieved / NOMINAL_HBM_GBS, 4),
                          "traffic_source": traffic_src},

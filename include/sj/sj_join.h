@@ -562,7 +562,8 @@ SJ_EXPORT const char* sj_last_error(void);
 /* Opt-in per-kernel timing. While enabled (process-wide), every kernel the library launches from
  * the calling thread is bracketed by a CUDA event pair on its stream; sj_timing_collect waits for
  * those events, writes up to `capacity` (name, milliseconds) records in launch order, clears the
- * log and returns the number of records. Names are static strings. Off by default. */
+ * log and returns the number of records. Names are static strings. Off by default. Turning it on
+ * creates a pool of 512 events for the calling thread, so the timed launches create none. */
 typedef struct sj_kernel_time {
   const char* name;
   float ms;

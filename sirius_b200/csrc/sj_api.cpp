@@ -390,7 +390,16 @@ SJ_EXPORT const char* sj_status_string(sj_status s) {
 
 SJ_EXPORT const char* sj_last_error(void) { return g_last_error.c_str(); }
 
-SJ_EXPORT void sj_timing_enable(int32_t on) { g_timing.store(on != 0); }
+SJ_EXPORT void sj_timing_enable(int32_t on) {
+  // events for the calling thread's timed launches, made here rather than inside a timed region
+  if (on)
+    while (t_event_pool.size() < 512) {
+      cudaEvent_t e = nullptr;
+      if (cudaEventCreate(&e) != cudaSuccess) break;
+      t_event_pool.push_back(e);
+    }
+  g_timing.store(on != 0);
+}
 
 SJ_EXPORT int32_t sj_timing_collect(sj_kernel_time* out, int32_t capacity) {
   const int32_t n = (int32_t)t_records.size();

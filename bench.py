@@ -63,7 +63,7 @@ def parse():
     ap.add_argument("--e2e-chunk-rows", type=int, default=0, help="probe rows per chunk of the e2e host join")
     ap.add_argument("--table-l2", type=int, default=0, help="L2 priority of table loads: 0 auto, 1 normal, 2 evict_last")
     ap.add_argument("--ctas-per-sm", type=int, default=0)
-    ap.add_argument("--workload", default="large", choices=["large", "small", "skewed", "batched", "served"])
+    ap.add_argument("--workload", default="large", choices=["large", "small", "skewed", "batched", "served", "next"])
     ap.add_argument("--autotune", action="store_true", help="batched: choose launch parameters by the autotuner")
     ap.add_argument("--requests", type=int, default=2000)
     ap.add_argument("--slots", type=int, default=4)
@@ -461,11 +461,12 @@ def run_sj(args):
 
 
 def run_secondary(args):
-    """Records of the small, skewed, batched and served workloads (default sizes and seeds)."""
+    """Records of the small, skewed, batched and served workloads and of the rows after the INNER path
+    (join kinds, two-column keys, partition operator, dynamic filter), at default sizes and seeds."""
     import copy
     import torch
     recs = {}
-    for wl in ("small", "skewed", "batched", "served"):
+    for wl in ("small", "skewed", "batched", "served", "next"):
         a = copy.copy(args)
         a.workload = wl
         a.n_build = a.n_probe = None
@@ -474,7 +475,8 @@ def run_secondary(args):
         a.autotune = wl == "batched"
         t0 = time.perf_counter()
         try:
-            rec = run_batched(a) if wl == "batched" else run_served(a) if wl == "served" else run_other(a)
+            rec = (run_batched(a) if wl == "batched" else run_served(a) if wl == "served" else
+                   run_next(a) if wl == "next" else run_other(a))
             rec["bench_seconds"] = round(time.perf_counter() - t0, 1)
         except Exception as e:  # one workload's failure is reported in its record, the line still prints
             rec = {"error": f"{type(e).__name__}: {e}"}
@@ -950,6 +952,265 @@ def run_other(args):
     return line
 
 
+# --------------------------------------------------------------------------------------------
+# the rows after the INNER path: join kinds, two-column keys, the partition operator, the filter
+# --------------------------------------------------------------------------------------------
+def run_next(args):
+    """LEFT / SEMI / ANTI / MARK on the large table with 30 % of the probe keys absent, a two-column
+    int32 key, the hash partition operator and the dynamic filter, each timed on the device (CUDA
+    events, inputs resident, a short spin kernel ahead of each timed region) and checked against
+    an independent rule in the same run."""
+    import ctypes
+    import torch
+    from sirius_b200 import datagen as D
+    from sirius_b200 import join as J
+    from sirius_b200 import _lib as L
+    from oracle import oracle as O
+    lib = L.load()
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    stream = torch.cuda.current_stream()
+    sh = stream.cuda_stream
+    peak, peak_src = measured_peak()
+    steps = max(3, args.steps)
+
+    def timed(fn):
+        for _ in range(max(3, args.warmup)):
+            fn()
+        torch.cuda.synchronize()
+        torch.cuda._sleep(4_000_000)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(steps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / steps
+
+    def rec(rows, ms, alg, check, **extra):
+        a = alg / (ms / 1e3) / 1e9
+        return dict({"ms": round(ms, 4), "Mrows_per_s": round(rows / (ms / 1e3) / 1e6, 1),
+                     "alg_bytes": int(alg), "achieved_GBps": round(a, 1), "frac_of_peak": round(a / peak, 4),
+                     "oracle_check": check}, **extra)
+
+    out = {"peak": peak, "peak_source": peak_src, "steps": steps}
+    with ClockSampler(0) as clk:
+        # ---- 1. join kinds on the large table ----
+        nb, n = 16 << 20, 64 << 20
+        inp = D.large(args.seed, nb, n)
+        bk = torch.from_numpy(inp.build_keys).to(dev)
+        bp = [torch.from_numpy(c).to(dev) for c in inp.build_payload]
+        pk0 = torch.from_numpy(inp.probe_keys).to(dev)
+        pp = torch.from_numpy(inp.probe_payload[0]).to(dev)
+        g = torch.Generator(device=dev)
+        g.manual_seed(args.seed + 9)
+        miss = torch.rand(n, device=dev, generator=g) < 0.3
+        pk = torch.where(miss, pk0 + (1 << 41), pk0)  # build keys are < 2^40: these are absent
+        del pk0
+        hits = int((~miss).sum().item())
+        misses = n - hits
+        table = J.HashTable(bk, attach=bp)
+        kcols, nkeys, _ = J._keys(pk)
+        pin = J._cols([J.make_column(pp)])
+        dc = torch.zeros(1, dtype=torch.int64, device=dev)
+        cap_full = n + nb  # FULL: every probe row, plus at most every build row
+        words = (cap_full + 31) // 32
+        o_prid = torch.empty(cap_full, dtype=torch.int32, device=dev)
+        o_brid = torch.empty(cap_full, dtype=torch.int32, device=dev)
+        o_pp = torch.empty(cap_full, dtype=torch.int64, device=dev)
+        o_pv = torch.empty(words, dtype=torch.int32, device=dev)
+        o_bp = [torch.empty(cap_full, dtype=torch.int64, device=dev) for _ in bp]
+        o_bv = [torch.empty(words, dtype=torch.int32, device=dev) for _ in bp]
+        o_mark = torch.empty(n, dtype=torch.uint8, device=dev)
+        o_markv = torch.empty(words, dtype=torch.int32, device=dev)
+        pout = J._cols([J._mut(o_pp, None)], L.SjMutColumn)
+        pout_full = J._cols([J._mut(o_pp, o_pv)], L.SjMutColumn)
+        bin_full = J._cols([J.make_column(c) for c in bp])  # FULL gathers from the caller's columns
+        bout_left = J._cols([J._mut(t, v) for t, v in zip(o_bp, o_bv)], L.SjMutColumn)
+        bout_inner = J._cols([J._mut(t, None) for t in o_bp], L.SjMutColumn)
+
+        def kind(k):
+            def f():
+                if k == L.SJ_JOIN_INNER:
+                    L.check(lib.sj_probe_gather(table.handle, kcols, nkeys, pin, 1, None, len(bp), o_prid.data_ptr(),
+                                                o_brid.data_ptr(), pout, bout_inner, n, None, sh, dc.data_ptr()),
+                            "sj_probe_gather")
+                    return
+                full = k == L.SJ_JOIN_FULL
+                left, mark = k == L.SJ_JOIN_LEFT or full, k == L.SJ_JOIN_MARK
+                L.check(lib.sj_probe_join(table.handle, k, kcols, nkeys, None if mark else pin, 0 if mark else 1,
+                                          bin_full if full else None, len(bp) if left else 0,
+                                          None if mark else o_prid.data_ptr(),
+                                          o_brid.data_ptr() if left else None,
+                                          None if mark else pout_full if full else pout,
+                                          bout_left if left else None, 0 if mark else cap_full if full else n,
+                                          o_mark.data_ptr() if mark else None, o_markv.data_ptr() if mark else None,
+                                          None, sh, dc.data_ptr()), "sj_probe_join")
+            return f
+
+        sample = torch.randint(0, n, (1 << 20,), device=dev, generator=g)
+        kinds = {}
+        key_in = 8 * n
+        # INNER
+        ms = timed(kind(L.SJ_JOIN_INNER))
+        c = int(dc.item())
+        s = sample[sample < c]
+        ok = c == hits and torch.equal(pk[o_prid[s].long()], bk[o_brid[s].long()])
+        assert ok, "inner: count or joined keys differ"
+        kinds["inner"] = rec(n, ms, key_in + 8 * hits + 32 * hits + 16 * nb,
+                             {"kind": "count = probe rows whose key is in the build; sampled rows join equal keys",
+                              "rows": c, "passed": True})
+        # LEFT
+        ms = timed(kind(L.SJ_JOIN_LEFT))
+        c = int(dc.item())
+        nr = o_brid[:c] == L.SJ_NO_ROW
+        s = sample[sample < c]
+        sb = o_brid[s]
+        ok = (c == n and int(nr.sum().item()) == misses and torch.equal(miss[o_prid[:c].long()], nr)
+              and torch.equal(pk[o_prid[s].long()][sb != L.SJ_NO_ROW], bk[sb[sb != L.SJ_NO_ROW].long()]))
+        assert ok, "left: rows differ"
+        kinds["left"] = rec(n, ms, key_in + 8 * n + n * 32 + 2 * n // 8 + 16 * nb,
+                            {"kind": "every probe row once; no build row exactly for the absent keys; sampled "
+                                     "matched rows join equal keys", "rows": c, "passed": True})
+        # SEMI
+        ms = timed(kind(L.SJ_JOIN_SEMI))
+        c = int(dc.item())
+        ok = c == hits and not bool(miss[o_prid[:c].long()].any())
+        assert ok, "semi: rows differ"
+        kinds["semi"] = rec(n, ms, key_in + (8 + 12) * hits,
+                            {"kind": "exactly the probe rows whose key is in the build", "rows": c, "passed": True})
+        # ANTI
+        ms = timed(kind(L.SJ_JOIN_ANTI))
+        c = int(dc.item())
+        ok = c == misses and bool(miss[o_prid[:c].long()].all())
+        assert ok, "anti: rows differ"
+        kinds["anti"] = rec(n, ms, key_in + (8 + 12) * misses,
+                            {"kind": "exactly the probe rows whose key is absent", "rows": c, "passed": True})
+        # MARK
+        ms = timed(kind(L.SJ_JOIN_MARK))
+        ok = torch.equal(o_mark.bool(), ~miss)
+        assert ok, "mark: marks differ"
+        kinds["mark"] = rec(n, ms, key_in + n + n // 8,
+                            {"kind": "mark byte of every probe row equals key-in-build", "rows": n, "passed": True})
+        # FULL
+        ms = timed(kind(L.SJ_JOIN_FULL))
+        c = int(dc.item())
+        hit_keys = torch.unique(pk[~miss])
+        unmatched_build = int((~torch.isin(bk, hit_keys)).sum().item())
+        del hit_keys
+        ok = c == n + unmatched_build
+        ok = ok and int((o_prid[:c] == L.SJ_NO_ROW).sum().item()) == unmatched_build
+        ok = ok and int((o_brid[:c] == L.SJ_NO_ROW).sum().item()) == misses
+        assert ok, "full: rows differ"
+        kinds["full"] = rec(n, ms, key_in + 8 * n + c * 32 + 3 * c // 8 + 16 * nb,
+                            {"kind": "probe rows + build rows no probe row matched; padded rows are exactly the "
+                                     "absent probe keys and the unmatched build keys", "rows": c,
+                             "unmatched_build_rows": unmatched_build, "passed": True})
+        out["join_kinds"] = {"workload": f"build {nb} unique int64 keys + 2 int64 payloads (attached, partitioned "
+                                         f"table); probe {n} int64 keys, 30 % absent from the build, + 1 int64 "
+                                         f"payload", "probe_rows": n, "hits": hits, **kinds}
+        # ---- 4. the dynamic filter: filled by the insert pass, tested against the probe keys ----
+        t_plain, t_bloom = [], []
+        bt = None
+        for _ in range(3):
+            for bits, acc in ((0, t_plain), (16, t_bloom)):
+                torch.cuda.synchronize()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record()
+                tb = J.HashTable(bk, attach=bp, bloom_bits_per_key=bits)
+                e1.record()
+                torch.cuda.synchronize()
+                acc.append(e0.elapsed_time(e1))
+                if bits:
+                    if bt is not None:
+                        bt.close()
+                    bt = tb
+                else:
+                    tb.close()
+        bloom = bt.bloom()
+        mask = torch.empty(n, dtype=torch.uint8, device=dev)
+        pcol = J.make_column(pk)
+
+        def contains():
+            L.check(lib.sj_bloom_contains(bloom._h, ctypes.byref(pcol), mask.data_ptr(), None, sh), "sj_bloom_contains")
+
+        ms = timed(contains)
+        fneg = int((~mask.bool() & ~miss).sum().item())
+        fpr = float(mask[miss].float().mean().item())
+        assert fneg == 0 and fpr < 0.01, f"filter: {fneg} false negatives, false-positive rate {fpr}"
+        out["dynamic_filter"] = {
+            "workload": f"filter of {nb} build keys at 16 bits per key, filled by the table's insert pass; "
+                        f"tested against the {n} probe keys above",
+            "build_ms_without": round(min(t_plain), 3), "build_ms_with_filter": round(min(t_bloom), 3),
+            "filter_bytes": bloom.nbytes,
+            "contains": rec(n, ms, 8 * n + n + bloom.nbytes,
+                            {"kind": "no false negatives over every present key; false-positive rate over the "
+                                     "absent keys", "false_positive_rate": round(fpr, 6), "passed": True})}
+        bt.close()
+        table.close()
+        del o_bp, o_bv, o_pp, o_pv, o_brid, o_prid, o_mark, mask
+        torch.cuda.empty_cache()
+        # ---- 3. the partition operator on the probe side ----
+        P = 64
+        kpart = J._keys(pk)[0]
+        ins = J._cols([J.make_column(pk), J.make_column(pp)])
+        p_keys = torch.empty(n, dtype=torch.int64, device=dev)
+        p_pay = torch.empty(n, dtype=torch.int64, device=dev)
+        p_outs = J._cols([J._mut(p_keys, None), J._mut(p_pay, None)], L.SjMutColumn)
+        offs = torch.empty(P + 1, dtype=torch.int64, device=dev)
+
+        def part():
+            L.check(lib.sj_hash_partition(kpart, 1, ins, 2, P, p_outs, offs.data_ptr(), None, sh), "sj_hash_partition")
+
+        ms = timed(part)
+        off = offs.cpu().numpy()
+        ok = off[0] == 0 and off[-1] == n and bool(np.all(np.diff(off) >= 0))
+        ok = ok and int(p_keys.sum().item()) == int(pk.sum().item())  # the same multiset of keys (sum)
+        pos = np.sort(np.random.default_rng(args.seed).choice(n, 1 << 20, replace=False))
+        kk = p_keys[torch.from_numpy(pos).to(dev)].cpu().numpy()
+        want = O.partition_ids([kk], [None], P)
+        got = np.searchsorted(off, pos, side="right") - 1
+        ok = ok and bool(np.array_equal(want, got))
+        assert ok, "partition: rows in the wrong partition"
+        out["partition_operator"] = {
+            "workload": f"{n} int64 keys + 1 int64 payload (the probe side above) into {P} partitions",
+            **rec(n, ms, 32 * n + 8 * (P + 1),
+                  {"kind": "offsets cover every row; the key multiset is kept (sum); 2^20 sampled rows lie in "
+                           "the partition the oracle's partition rule gives them", "rows": n, "passed": True})}
+        del p_keys, p_pay, pk, pp, miss
+        torch.cuda.empty_cache()
+        # ---- 2. two int32 key columns ----
+        nb2, n2 = 8 << 20, 32 << 20
+        r = np.random.default_rng(args.seed + 11)
+        codes = r.permutation(1 << 24)[:nb2]
+        k1, k2 = (codes >> 11).astype(np.int32), (codes & 2047).astype(np.int32)
+        idx = r.integers(0, nb2, n2)
+        b1, b2 = torch.from_numpy(k1).to(dev), torch.from_numpy(k2).to(dev)
+        q1, q2 = torch.from_numpy(k1[idx]).to(dev), torch.from_numpy(k2[idx]).to(dev)
+        t2 = J.HashTable([b1, b2])
+        mk, mn, _ = J._keys([q1, q2])
+        m_prid = torch.empty(n2, dtype=torch.int32, device=dev)
+        m_brid = torch.empty(n2, dtype=torch.int32, device=dev)
+
+        def multikey():
+            L.check(lib.sj_probe_gather(t2.handle, mk, mn, None, 0, None, 0, m_prid.data_ptr(), m_brid.data_ptr(),
+                                        None, None, n2, None, sh, dc.data_ptr()), "sj_probe_gather")
+
+        ms = timed(multikey)
+        c = int(dc.item())
+        s = torch.randint(0, n2, (1 << 20,), device=dev)
+        pr, br = m_prid[s].long(), m_brid[s].long()
+        ok = c == n2 and torch.equal(q1[pr], b1[br]) and torch.equal(q2[pr], b2[br])
+        assert ok, "two-column keys: rows differ"
+        out["multi_column_keys"] = {
+            "workload": f"build {nb2} unique (int32, int32) keys; probe {n2} rows drawn from them",
+            **rec(n2, ms, 8 * n2 + 8 * c,
+                  {"kind": "every probe row matches once; 2^20 sampled rows join equal key pairs", "rows": c,
+                   "passed": True})}
+        t2.close()
+    out["clocks"] = clk.summary()
+    return out
+
 def main():
     args = parse()
     if args.workload == "large" or args.impl == "reference":
@@ -957,8 +1218,8 @@ def main():
         args.n_probe = args.n_probe or 64 << 20
     if args.impl == "reference":
         return run_reference(args)
-    if args.workload in ("batched", "served", "small", "skewed"):
-        runner = {"batched": run_batched, "served": run_served}.get(args.workload, run_other)
+    if args.workload in ("batched", "served", "small", "skewed", "next"):
+        runner = {"batched": run_batched, "served": run_served, "next": run_next}.get(args.workload, run_other)
         print(json.dumps(runner(args)), flush=True)
         return 0
     return run_sj(args)

@@ -4,8 +4,12 @@
 // resolve_mark_join_result, :1461-1525).
 //
 //   SEMI / ANTI  one pass: every probe row looks its key up (a NULL key finds nothing unless NULLs
-//                compare equal and the build has NULL keys) and the selected rows are compacted
-//                warp-aggregated (ballot rank + one atomicAdd per warp) with their probe payloads.
+//                compare equal and the build has NULL keys) and the selected rows are compacted with
+//                their probe payloads. A warp stages the selected row ids in shared memory and
+//                reserves output once per flush of about 224 rows, then writes rows and payloads in
+//                contiguous runs: one atomicAdd per 32-row step on the one output counter serialised
+//                the pass (64M rows, 30 % absent: ANTI 2.60 ms, MARK — the same lookups without
+//                compaction — 0.85 ms).
 //   MARK         one pass, no compaction: mark byte and validity bit of every probe row. Unmatched
 //                rows are NULL when their key is NULL, or all of them when the build has a NULL key.
 //   LEFT         the INNER probe + gather (probe_gather, any table layout), then the ANTI pass
@@ -25,6 +29,7 @@ namespace sj {
 TableDev table_dev(const sj_table* t);
 
 constexpr int kKindThreads = 256;
+constexpr int kKindStage = 256;  // staged row ids per warp (SEMI / ANTI rows, FULL's unmatched build rows)
 constexpr int32_t kNoRow = (int32_t)0x80000000;
 
 enum KindMode { kSemi = 0, kAnti = 1, kMark = 2, kFlags = 3 };
@@ -86,6 +91,29 @@ __global__ void __launch_bounds__(kKindThreads) kind_probe_kernel(TableDev t, co
   const int lane = threadIdx.x & 31;
   const unsigned below = (1u << lane) - 1u;
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  __shared__ int32_t s_stage[kKindThreads / 32][kKindStage];
+  int32_t* st = s_stage[threadIdx.x >> 5];
+  uint32_t fill = 0;  // staged rows of this warp (warp-uniform)
+  // reserve the staged rows' output range with one atomicAdd and write them out in order
+  auto flush = [&]() {
+    __syncwarp();
+    unsigned long long base = 0;
+    if (lane == 0) base = atomicAdd(a.d_count, (unsigned long long)fill);
+    base = __shfl_sync(kFullMask, base, 0);
+    for (uint32_t e = lane; e < fill; e += 32) {
+      const int64_t p = (int64_t)base + e;
+      if (p >= a.capacity) break;
+      const int64_t i = st[e];
+      if (a.out_prid) a.out_prid[p] = (int32_t)i;
+      if (a.out_brid) a.out_brid[p] = kNoRow;
+      for (int c = 0; c < a.n_pin; ++c) {
+        store_elem(a.pout[c].data, p, a.pin[c].width, pl_load(a.pin[c], i));
+        if (a.pout[c].valid && payload_valid(a.pin[c], i)) set_out_bit(a.pout[c].valid, p);
+      }
+    }
+    __syncwarp();
+    fill = 0;
+  };
   for (int64_t i0 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) & ~31ll; i0 < n; i0 += stride) {
     const int64_t i = i0 + lane;
     const bool live = i < n;
@@ -107,19 +135,12 @@ __global__ void __launch_bounds__(kKindThreads) kind_probe_kernel(TableDev t, co
     const bool sel = live && (MODE == kSemi ? found : !found);
     const unsigned bal = __ballot_sync(kFullMask, sel);
     if (!bal) continue;
-    unsigned long long base = 0;
-    if (lane == 0) base = atomicAdd(a.d_count, (unsigned long long)__popc(bal));
-    base = __shfl_sync(kFullMask, base, 0);
-    const int64_t p = (int64_t)base + __popc(bal & below);
-    if (sel && p < a.capacity) {
-      if (a.out_prid) a.out_prid[p] = (int32_t)i;
-      if (a.out_brid) a.out_brid[p] = kNoRow;
-      for (int c = 0; c < a.n_pin; ++c) {
-        store_elem(a.pout[c].data, p, a.pin[c].width, pl_load(a.pin[c], i));
-        if (a.pout[c].valid && payload_valid(a.pin[c], i)) set_out_bit(a.pout[c].valid, p);
-      }
-    }
+    if (sel) st[fill + __popc(bal & below)] = (int32_t)i;
+    fill += __popc(bal);
+    if (fill > (uint32_t)(kKindStage - 32)) flush();  // the next step could not fit
   }
+  if (MODE == kSemi || MODE == kAnti)
+    if (fill) flush();
 }
 
 struct BuildEmitArgs {
@@ -135,22 +156,43 @@ struct BuildEmitArgs {
   const uint8_t* flags;
 };
 
-__device__ __forceinline__ void emit_build_row(const BuildEmitArgs& a, bool sel, int32_t brid) {
-  const int lane = threadIdx.x & 31;
-  const unsigned bal = __ballot_sync(kFullMask, sel);
-  if (!bal) return;
-  unsigned long long base = 0;
-  if (lane == 0) base = atomicAdd(a.d_count, (unsigned long long)__popc(bal));
-  base = __shfl_sync(kFullMask, base, 0);
-  const int64_t p = (int64_t)base + __popc(bal & ((1u << lane) - 1u));
-  if (!sel || p >= a.capacity) return;
-  if (a.out_prid) a.out_prid[p] = kNoRow;
-  if (a.out_brid) a.out_brid[p] = brid;
-  for (int c = 0; c < a.n_bin; ++c) {
-    store_elem(a.bout[c].data, p, a.bin[c].width, pl_load(a.bin[c], brid));
-    if (a.bout[c].valid && payload_valid(a.bin[c], brid)) set_out_bit(a.bout[c].valid, p);
+// Unmatched build rows of a FULL join, staged per warp like the SEMI / ANTI rows: build row ids
+// collect in the warp's shared-memory area, and a flush reserves their output range with one
+// atomicAdd and writes them (probe row id SJ_NO_ROW, build row id, build payloads) in order.
+struct BuildEmitter {
+  const BuildEmitArgs& a;
+  int32_t* st;        // this warp's kKindStage staged build row ids
+  uint32_t fill = 0;  // warp-uniform
+  __device__ BuildEmitter(const BuildEmitArgs& args, int32_t* stage) : a(args), st(stage) {}
+  __device__ void add(bool sel, int32_t brid) {
+    const int lane = threadIdx.x & 31;
+    const unsigned bal = __ballot_sync(kFullMask, sel);
+    if (!bal) return;
+    if (sel) st[fill + __popc(bal & ((1u << lane) - 1u))] = brid;
+    fill += __popc(bal);
+    if (fill > (uint32_t)(kKindStage - 32)) flush();
   }
-}
+  __device__ void flush() {
+    const int lane = threadIdx.x & 31;
+    __syncwarp();
+    unsigned long long base = 0;
+    if (lane == 0 && fill) base = atomicAdd(a.d_count, (unsigned long long)fill);
+    base = __shfl_sync(kFullMask, base, 0);
+    for (uint32_t e = lane; e < fill; e += 32) {
+      const int64_t p = (int64_t)base + e;
+      if (p >= a.capacity) break;
+      const int32_t brid = st[e];
+      if (a.out_prid) a.out_prid[p] = kNoRow;
+      if (a.out_brid) a.out_brid[p] = brid;
+      for (int c = 0; c < a.n_bin; ++c) {
+        store_elem(a.bout[c].data, p, a.bin[c].width, pl_load(a.bin[c], brid));
+        if (a.bout[c].valid && payload_valid(a.bin[c], brid)) set_out_bit(a.bout[c].valid, p);
+      }
+    }
+    __syncwarp();
+    fill = 0;
+  }
+};
 
 __device__ __forceinline__ int32_t rid_of_pos(const BuildEmitArgs& a, int64_t pos) {
   return a.pos_rid ? __ldg(reinterpret_cast<const int32_t*>(reinterpret_cast<const char*>(a.pos_rid) +
@@ -164,6 +206,8 @@ __global__ void __launch_bounds__(kKindThreads) unmatched_slots_kernel(TableDev 
   using Ops = SlotOps<WIDE>;
   const int lane = threadIdx.x & 31;
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  __shared__ int32_t s_stage[kKindThreads / 32][kKindStage];
+  BuildEmitter em(a, s_stage[threadIdx.x >> 5]);
   for (int64_t i0 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) & ~31ll; i0 < n_slots; i0 += stride) {
     const int64_t i = i0 + lane;
     bool sel = false;
@@ -176,8 +220,9 @@ __global__ void __launch_bounds__(kKindThreads) unmatched_slots_kernel(TableDev 
         brid = rid_of_pos(a, Ops::rid(bk, q, t.rbits));
       }
     }
-    emit_build_row(a, sel, brid);
+    em.add(sel, brid);
   }
+  em.flush();
 }
 
 // FULL, GROUPED table: member i (group order) belongs to the last group s with grp_off[s] <= i.
@@ -185,6 +230,8 @@ __global__ void __launch_bounds__(kKindThreads) unmatched_members_kernel(TableDe
                                                                          int64_t n_groups, BuildEmitArgs a) {
   const int lane = threadIdx.x & 31;
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  __shared__ int32_t s_stage[kKindThreads / 32][kKindStage];
+  BuildEmitter em(a, s_stage[threadIdx.x >> 5]);
   for (int64_t i0 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) & ~31ll; i0 < n_members; i0 += stride) {
     const int64_t i = i0 + lane;
     bool sel = false;
@@ -201,18 +248,22 @@ __global__ void __launch_bounds__(kKindThreads) unmatched_members_kernel(TableDe
         brid = rid_of_pos(a, t.grp_rid ? (int64_t)__ldg(t.grp_rid + i) : i);
       }
     }
-    emit_build_row(a, sel, brid);
+    em.add(sel, brid);
   }
+  em.flush();
 }
 
 // FULL: the NULL-key build rows (not in the table when NULLs never match).
 __global__ void __launch_bounds__(kKindThreads) null_build_rows_kernel(const int32_t* __restrict__ null_rid,
                                                                        int64_t n_null, BuildEmitArgs a) {
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  __shared__ int32_t s_stage[kKindThreads / 32][kKindStage];
+  BuildEmitter em(a, s_stage[threadIdx.x >> 5]);
   for (int64_t i0 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) & ~31ll; i0 < n_null; i0 += stride) {
     const int64_t i = i0 + (threadIdx.x & 31);
-    emit_build_row(a, i < n_null, i < n_null ? __ldg(null_rid + i) : 0);
+    em.add(i < n_null, i < n_null ? __ldg(null_rid + i) : 0);
   }
+  em.flush();
 }
 
 // Sets validity bits [lo, hi) (bounds read from the device, clamped to cap; lo_p NULL = 0).

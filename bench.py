@@ -974,10 +974,14 @@ def run_next(args):
     peak, peak_src = measured_peak()
     steps = max(3, args.steps)
 
+    last_kernels = {}
+
     def timed(fn):
         for _ in range(max(3, args.warmup)):
             fn()
         torch.cuda.synchronize()
+        L.timing_collect()
+        L.timing_enable(True)
         torch.cuda._sleep(4_000_000)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
@@ -985,13 +989,19 @@ def run_next(args):
             fn()
         e1.record()
         torch.cuda.synchronize()
+        L.timing_enable(False)
+        per = {}
+        for name, kms in L.timing_collect():
+            per[name] = per.get(name, 0.0) + kms
+        last_kernels.clear()
+        last_kernels.update({k: round(v / steps, 4) for k, v in sorted(per.items(), key=lambda kv: -kv[1])})
         return e0.elapsed_time(e1) / steps
 
     def rec(rows, ms, alg, check, **extra):
         a = alg / (ms / 1e3) / 1e9
         return dict({"ms": round(ms, 4), "Mrows_per_s": round(rows / (ms / 1e3) / 1e6, 1),
                      "alg_bytes": int(alg), "achieved_GBps": round(a, 1), "frac_of_peak": round(a / peak, 4),
-                     "oracle_check": check}, **extra)
+                     "kernels_ms": dict(last_kernels), "oracle_check": check}, **extra)
 
     out = {"peak": peak, "peak_source": peak_src, "steps": steps}
     with ClockSampler(0) as clk:

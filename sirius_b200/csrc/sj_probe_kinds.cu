@@ -12,9 +12,12 @@
 //                compaction — 0.85 ms).
 //   MARK         one pass, no compaction: mark byte and validity bit of every probe row. Unmatched
 //                rows are NULL when their key is NULL, or all of them when the build has a NULL key.
-//   LEFT         the INNER probe + gather (probe_gather, any table layout), then the ANTI pass
-//                appending the unmatched probe rows after the INNER rows on the same counter with
-//                build row id SJ_NO_ROW; validity of the NULL-padded build payloads is set by range.
+//   LEFT         the INNER probe + gather (probe_gather, any table layout), then the unmatched probe
+//                rows appended after the INNER rows on the same counter with build row id
+//                SJ_NO_ROW: the rows whose bit is clear in a mask set from the INNER rows' probe row
+//                ids (or, when no probe row ids are written or the INNER rows overflowed the
+//                capacity, the ANTI lookup); validity of the NULL-padded build payloads is set by
+//                range.
 //   FULL         LEFT, then a pass that flags every table slot (group) some probe row matched, then
 //                the unmatched build rows: a DISTINCT table walks its slots, a GROUPED table its
 //                group-ordered members (group of member i = the last group starting at or before i),
@@ -32,7 +35,7 @@ constexpr int kKindThreads = 256;
 constexpr int kKindStage = 256;  // staged row ids per warp (SEMI / ANTI rows, FULL's unmatched build rows)
 constexpr int32_t kNoRow = (int32_t)0x80000000;
 
-enum KindMode { kSemi = 0, kAnti = 1, kMark = 2, kFlags = 3 };
+enum KindMode { kSemi = 0, kAnti = 1, kMark = 2, kFlags = 3, kUnmatched = 4 };
 
 struct KindArgs {
   int32_t* out_prid;
@@ -46,6 +49,9 @@ struct KindArgs {
   uint32_t* mark_valid;
   int32_t build_has_null;
   uint8_t* flags;  // kFlags: one byte per slot (+ the NULL group)
+  const uint32_t* matched;  // kUnmatched: bit i set when probe row i has an INNER row
+  const unsigned long long* inner_rows;  // kUnmatched: INNER rows; past `capacity` the bits are
+                                         // incomplete and the rows are looked up instead
 };
 
 // Slot of key k in the table (k in range), or -1. Slots fill each bucket in order, so the walk stops
@@ -94,6 +100,7 @@ __global__ void __launch_bounds__(kKindThreads) kind_probe_kernel(TableDev t, co
   __shared__ int32_t s_stage[kKindThreads / 32][kKindStage];
   int32_t* st = s_stage[threadIdx.x >> 5];
   uint32_t fill = 0;  // staged rows of this warp (warp-uniform)
+  const bool by_bits = MODE == kUnmatched && (int64_t)*a.inner_rows <= a.capacity;
   // reserve the staged rows' output range with one atomicAdd and write them out in order
   auto flush = [&]() {
     __syncwarp();
@@ -117,8 +124,14 @@ __global__ void __launch_bounds__(kKindThreads) kind_probe_kernel(TableDev t, co
   for (int64_t i0 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) & ~31ll; i0 < n; i0 += stride) {
     const int64_t i = i0 + lane;
     const bool live = i < n;
-    const bool valid = live && bit_valid(kv, kvoff, i);
-    const int64_t s = live ? lookup<K, WIDE>(t, __ldg(keys + i), valid) : -1;
+    int64_t s = -1;
+    const bool valid = live && (by_bits || bit_valid(kv, kvoff, i));
+    if (by_bits) {
+      // no lookup: the INNER rows already told which probe rows matched
+      if (live && (__ldg(a.matched + (i >> 5)) >> (i & 31) & 1u)) s = 0;
+    } else {
+      s = live ? lookup<K, WIDE>(t, __ldg(keys + i), valid) : -1;
+    }
     const bool found = s >= 0;
     if (MODE == kMark) {
       if (live) a.mark[i] = found ? 1 : 0;
@@ -132,14 +145,14 @@ __global__ void __launch_bounds__(kKindThreads) kind_probe_kernel(TableDev t, co
       if (found) a.flags[s] = 1;
       continue;
     }
-    const bool sel = live && (MODE == kSemi ? found : !found);
+    const bool sel = live && (MODE == kSemi ? found : !found);  // kAnti / kUnmatched: the rest
     const unsigned bal = __ballot_sync(kFullMask, sel);
     if (!bal) continue;
     if (sel) st[fill + __popc(bal & below)] = (int32_t)i;
     fill += __popc(bal);
     if (fill > (uint32_t)(kKindStage - 32)) flush();  // the next step could not fit
   }
-  if (MODE == kSemi || MODE == kAnti)
+  if (MODE == kSemi || MODE == kAnti || MODE == kUnmatched)
     if (fill) flush();
 }
 
@@ -286,6 +299,16 @@ __global__ void set_count_kernel(int64_t* d_count, int64_t v) { *d_count = v; }
 // ------------------------------------------------------------------------------------------------
 // host side
 // ------------------------------------------------------------------------------------------------
+// LEFT / FULL: bit r of `bits` for every probe row r among the first min(*d_n, cap) INNER rows.
+__global__ void __launch_bounds__(256) matched_bits_kernel(const int32_t* __restrict__ prid,
+                                                           const unsigned long long* d_n, int64_t cap, uint32_t* bits) {
+  const int64_t n = (int64_t)*d_n < cap ? (int64_t)*d_n : cap;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const uint32_t r = (uint32_t)__ldg(prid + i);
+    atomicOr(bits + (r >> 5), 1u << (r & 31));
+  }
+}
+
 static int kind_grid(const sj_table* t, int64_t n) {
   const int64_t need = (n + kKindThreads - 1) / kKindThreads;
   return (int)std::max<int64_t>(1, std::min<int64_t>(need, (int64_t)sm_count(t->device) * 8));
@@ -296,7 +319,8 @@ static void launch_kind(const sj_table* t, const sj_column& p, const KindArgs& a
   const int grid = kind_grid(t, p.num_rows);
   const TableDev d = table_dev(t);
   const bool wide = t->slot_kind == SJ_SLOT_WIDE128;
-  KernelTimer timer(MODE == kMark ? "mark" : MODE == kFlags ? "match_flags" : MODE == kSemi ? "semi" : "anti", s);
+  KernelTimer timer(MODE == kMark ? "mark" : MODE == kFlags ? "match_flags" : MODE == kSemi ? "semi"
+                    : MODE == kUnmatched ? "unmatched_probe" : "anti", s);
   if (t->key_type == SJ_INT32) {
     if (wide) kind_probe_kernel<int32_t, true, MODE><<<grid, kKindThreads, 0, s>>>(d, static_cast<const int32_t*>(p.data), p.validity, p.validity_offset, p.num_rows, a);
     else kind_probe_kernel<int32_t, false, MODE><<<grid, kKindThreads, 0, s>>>(d, static_cast<const int32_t*>(p.data), p.validity, p.validity_offset, p.num_rows, a);
@@ -394,10 +418,29 @@ sj_status probe_join(const sj_table* t, int32_t kind, const sj_column& p, const 
   // 1. INNER rows
   SJ_TRY(probe_gather(t, p, gs, alloc, s, d_count));
   SJ_CUDA_TRY(cudaMemcpyAsync(m, d_count, sizeof(int64_t), cudaMemcpyDeviceToDevice, s));
-  // 2. unmatched probe rows, appended
+  // 2. unmatched probe rows, appended: the probe rows no INNER row names (one bit per probe row, set
+  // from the INNER rows' probe row ids; 0.94 ms for a second lookup of 64M rows before), or a second
+  // lookup when the call writes no probe row ids
   a.out_prid = gs.out_probe_rid;
   a.out_brid = gs.out_build_rid;
-  if (p.num_rows > 0) launch_kind<kAnti>(t, p, a, s);
+  Scratch mbits;
+  if (p.num_rows > 0) {
+    if (gs.out_probe_rid && gs.capacity > 0) {
+      const size_t words = (size_t)((p.num_rows + 31) / 32);
+      SJ_TRY(mbits.get(alloc, words * sizeof(uint32_t), s));
+      SJ_CUDA_TRY(cudaMemsetAsync(mbits.ptr, 0, words * sizeof(uint32_t), s));
+      {
+        KernelTimer timer("matched_bits", s);
+        matched_bits_kernel<<<kind_grid(t, std::min<int64_t>(gs.capacity, p.num_rows)), 256, 0, s>>>(
+            gs.out_probe_rid, m, gs.capacity, mbits.as<uint32_t>());
+      }
+      a.matched = mbits.as<uint32_t>();
+      a.inner_rows = m;
+      launch_kind<kUnmatched>(t, p, a, s);
+    } else {
+      launch_kind<kAnti>(t, p, a, s);
+    }
+  }
   SJ_CUDA_TRY(cudaMemcpyAsync(m + 1, d_count, sizeof(int64_t), cudaMemcpyDeviceToDevice, s));
 
   // 3. FULL: unmatched build rows

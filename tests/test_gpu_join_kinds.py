@@ -213,3 +213,61 @@ def test_right_family_matches_oracle(cuda, kind, dup):
     # the swapped join: left is the build side, right the probe side
     inner = {J.JOIN_RIGHT: "left", J.JOIN_RIGHT_SEMI: "semi", J.JOIN_RIGHT_ANTI: "anti"}[kind]
     _check_rows(inner, out, lk, rk, lv, rv, [lp] if kind == J.JOIN_RIGHT else [], [rp])
+
+
+def _left_raw(t, pk, pp, capacity, dev):
+    """sj_probe_join LEFT with probe row ids, build row ids and caller-sized outputs; returns the
+    device count and the outputs (no capacity check)."""
+    lib = L.load()
+    kcols, nkeys, _ = J._keys(pk)
+    words = (capacity + 31) // 32
+    prid = torch.empty(capacity, dtype=torch.int32, device=dev)
+    brid = torch.empty(capacity, dtype=torch.int32, device=dev)
+    pout = torch.empty(capacity, dtype=pp.dtype, device=dev)
+    bouts = [torch.empty(capacity, dtype=c.dtype, device=dev) for c, _ in t.attached]
+    bvs = [torch.empty(words, dtype=torch.int32, device=dev) for _ in t.attached]
+    dc = torch.zeros(1, dtype=torch.int64, device=dev)
+    L.check(lib.sj_probe_join(t.handle, L.SJ_JOIN_LEFT, kcols, nkeys, J._cols([J.make_column(pp)]), 1, None,
+                              len(t.attached), prid.data_ptr(), brid.data_ptr(),
+                              J._cols([J._mut(pout, None)], L.SjMutColumn),
+                              J._cols([J._mut(b, v) for b, v in zip(bouts, bvs)], L.SjMutColumn), capacity,
+                              None, None, None, None, dc.data_ptr()), "sj_probe_join")
+    torch.cuda.synchronize()
+    return int(dc.item()), prid, brid, pout, bouts, bvs
+
+
+@pytest.mark.parametrize("frac_absent", [0.0, 0.3, 1.0])
+def test_left_partitioned_plain_payloads(cuda, frac_absent):
+    """LEFT on a partitioned DISTINCT table with attached payloads without NULLs: the unmatched probe
+    rows come from a bitmask of the INNER rows' probe row ids. NULL probe keys are unmatched rows."""
+    rng = np.random.default_rng(41)
+    nb, np_ = 200_000, 700_001
+    bk = rng.permutation(nb * 3)[:nb].astype(np.int64)
+    pk = bk[rng.integers(0, nb, np_)]
+    absent = rng.random(np_) < frac_absent
+    pk = np.where(absent, pk + (1 << 40), pk).astype(np.int64)
+    pv = O.pack_validity(rng.random(np_) > 0.02)
+    bp = [rng.integers(-2**40, 2**40, nb).astype(np.int64), rng.integers(-2**30, 2**30, nb).astype(np.int64)]
+    pp = [rng.integers(-2**40, 2**40, np_).astype(np.int64)]
+    with J.HashTable(dev_t(bk, cuda), partition_bits=4, attach=[dev_t(c, cuda) for c in bp]) as t:
+        out = t.probe_join(L.SJ_JOIN_LEFT, dev_t(pk, cuda), dev_valid(pv, cuda), [dev_t(c, cuda) for c in pp],
+                           attached=True)
+    assert out.count == np_
+    _check_rows("left", out, bk, pk, None, pv, bp, pp)
+
+
+def test_left_count_exact_when_inner_rows_overflow(cuda):
+    """A capacity below the INNER rows: the INNER rows past it are not written, so the matched-row
+    bits would be incomplete; the unmatched pass then looks the rows up again and the LEFT count
+    stays exact (every probe row once for a DISTINCT table)."""
+    rng = np.random.default_rng(43)
+    nb, np_ = 150_000, 500_000
+    bk = rng.permutation(nb * 2)[:nb].astype(np.int64)
+    pk = np.where(rng.random(np_) < 0.2, bk[rng.integers(0, nb, np_)] + (1 << 40),
+                  bk[rng.integers(0, nb, np_)]).astype(np.int64)
+    bp = [rng.integers(0, 1 << 30, nb).astype(np.int64)]
+    pp = torch.from_numpy(rng.integers(0, 1 << 30, np_).astype(np.int64)).to(cuda)
+    with J.HashTable(dev_t(bk, cuda), partition_bits=4, attach=[dev_t(c, cuda) for c in bp]) as t:
+        full, *_ = _left_raw(t, dev_t(pk, cuda), pp, np_, cuda)
+        small, *_ = _left_raw(t, dev_t(pk, cuda), pp, np_ // 3, cuda)
+    assert full == np_ and small == np_

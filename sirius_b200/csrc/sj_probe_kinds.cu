@@ -101,6 +101,8 @@ __global__ void __launch_bounds__(kKindThreads) kind_probe_kernel(TableDev t, co
   int32_t* st = s_stage[threadIdx.x >> 5];
   uint32_t fill = 0;  // staged rows of this warp (warp-uniform)
   const bool by_bits = MODE == kUnmatched && (int64_t)*a.inner_rows <= a.capacity;
+  // FULL flags pass: not needed when the build-row bits of the INNER rows are complete
+  if (MODE == kFlags && a.inner_rows && (int64_t)*a.inner_rows <= a.capacity) return;
   // reserve the staged rows' output range with one atomicAdd and write them out in order
   auto flush = [&]() {
     __syncwarp();
@@ -167,7 +169,16 @@ struct BuildEmitArgs {
   int64_t capacity;
   unsigned long long* d_count;
   const uint8_t* flags;
+  // FULL by build-row bits: when set and the INNER rows fit the capacity, the unmatched build rows
+  // are the rows whose bit in `matched` is clear (unmatched_build_rows_kernel); the slot / member /
+  // NULL-row walks then do nothing
+  const unsigned long long* inner_rows;
+  const uint32_t* matched;
 };
+
+__device__ __forceinline__ bool full_by_bits(const BuildEmitArgs& a) {
+  return a.inner_rows != nullptr && (int64_t)*a.inner_rows <= a.capacity;
+}
 
 // Unmatched build rows of a FULL join, staged per warp like the SEMI / ANTI rows: build row ids
 // collect in the warp's shared-memory area, and a flush reserves their output range with one
@@ -221,6 +232,7 @@ __global__ void __launch_bounds__(kKindThreads) unmatched_slots_kernel(TableDev 
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
   __shared__ int32_t s_stage[kKindThreads / 32][kKindStage];
   BuildEmitter em(a, s_stage[threadIdx.x >> 5]);
+  if (full_by_bits(a)) return;  // unmatched_build_rows_kernel emits them
   for (int64_t i0 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) & ~31ll; i0 < n_slots; i0 += stride) {
     const int64_t i = i0 + lane;
     bool sel = false;
@@ -245,6 +257,7 @@ __global__ void __launch_bounds__(kKindThreads) unmatched_members_kernel(TableDe
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
   __shared__ int32_t s_stage[kKindThreads / 32][kKindStage];
   BuildEmitter em(a, s_stage[threadIdx.x >> 5]);
+  if (full_by_bits(a)) return;  // unmatched_build_rows_kernel emits them
   for (int64_t i0 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) & ~31ll; i0 < n_members; i0 += stride) {
     const int64_t i = i0 + lane;
     bool sel = false;
@@ -272,9 +285,24 @@ __global__ void __launch_bounds__(kKindThreads) null_build_rows_kernel(const int
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
   __shared__ int32_t s_stage[kKindThreads / 32][kKindStage];
   BuildEmitter em(a, s_stage[threadIdx.x >> 5]);
+  if (full_by_bits(a)) return;  // unmatched_build_rows_kernel emits them
   for (int64_t i0 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) & ~31ll; i0 < n_null; i0 += stride) {
     const int64_t i = i0 + (threadIdx.x & 31);
     em.add(i < n_null, i < n_null ? __ldg(null_rid + i) : 0);
+  }
+  em.flush();
+}
+
+// FULL by build-row bits: every build row (NULL keys included) whose bit is clear.
+__global__ void __launch_bounds__(kKindThreads) unmatched_build_rows_kernel(const uint32_t* __restrict__ matched,
+                                                                            int64_t nb, BuildEmitArgs a) {
+  if (!full_by_bits(a)) return;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  __shared__ int32_t s_stage[kKindThreads / 32][kKindStage];
+  BuildEmitter em(a, s_stage[threadIdx.x >> 5]);
+  for (int64_t i0 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) & ~31ll; i0 < nb; i0 += stride) {
+    const int64_t i = i0 + (threadIdx.x & 31);
+    em.add(i < nb && !(__ldg(matched + (i >> 5)) >> (i & 31) & 1u), (int32_t)i);
   }
   em.flush();
 }
@@ -443,15 +471,28 @@ sj_status probe_join(const sj_table* t, int32_t kind, const sj_column& p, const 
   }
   SJ_CUDA_TRY(cudaMemcpyAsync(m + 1, d_count, sizeof(int64_t), cudaMemcpyDeviceToDevice, s));
 
-  // 3. FULL: unmatched build rows
-  Scratch flags;
+  // 3. FULL: unmatched build rows. With build row ids written: the build rows no INNER row names
+  // (one bit per build row, set from the INNER rows' build row ids), else — or when the INNER rows
+  // overflowed the capacity, decided on the device — the slots (groups) no probe row matched
+  Scratch flags, bbits;
   if (full) {
     const int64_t ns = t->num_slots();
     const int64_t nflags = ns + 1;  // + the NULL group
     SJ_TRY(flags.get(alloc, (size_t)nflags, s));
     SJ_CUDA_TRY(cudaMemsetAsync(flags.ptr, 0, (size_t)nflags, s));
+    const bool bits_ok = gs.out_build_rid != nullptr && gs.capacity > 0 && t->build_rows > 0;
+    if (bits_ok) {
+      const size_t words = (size_t)((t->build_rows + 31) / 32);
+      SJ_TRY(bbits.get(alloc, words * sizeof(uint32_t), s));
+      SJ_CUDA_TRY(cudaMemsetAsync(bbits.ptr, 0, words * sizeof(uint32_t), s));
+      KernelTimer timer("matched_build_bits", s);
+      matched_bits_kernel<<<kind_grid(t, std::min<int64_t>(gs.capacity, p.num_rows)), 256, 0, s>>>(
+          gs.out_build_rid, m, gs.capacity, bbits.as<uint32_t>());
+    }
     KindArgs fa{};
     fa.flags = flags.as<uint8_t>();
+    fa.capacity = gs.capacity;
+    fa.inner_rows = bits_ok ? m : nullptr;  // the flags pass returns at once when the bits apply
     if (p.num_rows > 0) launch_kind<kFlags>(t, p, fa, s);
     BuildEmitArgs e{};
     e.out_prid = gs.out_probe_rid;
@@ -470,8 +511,12 @@ sj_status probe_join(const sj_table* t, int32_t kind, const sj_column& p, const 
     e.capacity = gs.capacity;
     e.d_count = dc;
     e.flags = fa.flags;
+    e.inner_rows = bits_ok ? m : nullptr;
+    e.matched = bits_ok ? bbits.as<uint32_t>() : nullptr;
     const TableDev d = table_dev(t);
     KernelTimer timer("unmatched_build", s);
+    if (bits_ok)
+      unmatched_build_rows_kernel<<<kind_grid(t, t->build_rows), kKindThreads, 0, s>>>(e.matched, t->build_rows, e);
     if (t->layout == SJ_LAYOUT_DISTINCT) {
       if (ns > 0) {
         if (t->slot_kind == SJ_SLOT_WIDE128) unmatched_slots_kernel<true><<<kind_grid(t, ns), kKindThreads, 0, s>>>(d, ns, e);

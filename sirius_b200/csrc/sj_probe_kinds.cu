@@ -18,10 +18,12 @@
 //                ids (or, when no probe row ids are written or the INNER rows overflowed the
 //                capacity, the ANTI lookup); validity of the NULL-padded build payloads is set by
 //                range.
-//   FULL         LEFT, then a pass that flags every table slot (group) some probe row matched, then
-//                the unmatched build rows: a DISTINCT table walks its slots, a GROUPED table its
-//                group-ordered members (group of member i = the last group starting at or before i),
-//                and the NULL-key build rows come from the table's NULL-row list.
+//   FULL         LEFT, then the unmatched build rows: the build rows whose bit is clear in a mask
+//                set from the INNER rows' build row ids (NULL-key rows included). When no build row
+//                ids are written or the INNER rows overflowed the capacity: a pass that flags every
+//                table slot (group) some probe row matched, then a DISTINCT table walks its slots, a
+//                GROUPED table its group-ordered members (group of member i = the last group starting
+//                at or before i), and the NULL-key build rows come from the table's NULL-row list.
 #include <algorithm>
 
 #include "sj_device.cuh"

@@ -863,9 +863,19 @@ def run_other(args):
     assert m == int(mult.sum().item()), "match count differs from the key multiplicities"
     out = J.allocate_output(m, pp, bp, dev)
     d_count = torch.zeros(1, dtype=torch.int64, device=dev)
+    # the C ABI call with its arguments built once: a step of 1M rows takes tens of microseconds, so
+    # rebuilding the ctypes arguments every call (the Python wrapper) would be timed instead
+    lib = _lib.load()
+    kcols, nkeys, _ = J._keys(pk, pv)
+    pin = J._cols([J.make_column(*J._as_pair(c)) for c in pp])
+    pout = J._cols([J._mut(t, v) for t, v in zip(out.probe_payload, out.probe_payload_validity)], _lib.SjMutColumn)
+    bout = J._cols([J._mut(t, v) for t, v in zip(out.build_payload, out.build_payload_validity)], _lib.SjMutColumn)
+    sh = torch.cuda.current_stream().cuda_stream
 
     def step():
-        tb.probe_gather(pk, pv, pp, attached=True, capacity=m, out=out, d_count=d_count, sync=False)
+        _lib.check(lib.sj_probe_gather(tb.handle, kcols, nkeys, pin, len(pp), None, len(bp), out.probe_rid.data_ptr(),
+                                       out.build_rid.data_ptr(), pout, bout, m, None, sh, d_count.data_ptr()),
+                   "sj_probe_gather")
 
     for _ in range(max(3, args.warmup)):
         step()
@@ -877,6 +887,7 @@ def run_other(args):
     _lib.timing_enable(True)
     with ClockSampler(0) as clk:
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda._sleep(4_000_000)  # the host queues the first steps before the start event
         e0.record()
         for _ in range(args.steps):
             step()

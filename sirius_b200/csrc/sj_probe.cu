@@ -864,7 +864,7 @@ static sj_status probe_partitioned(const sj_table* t, const sj_column& p, Gather
     SJ_TRY(local_partition(ps, t->key_type, pbits, pd, run_off, run_cnt, t->device, s));
     g.prid_map = pd.rid;
     for (int c = 0; c < g.n_pin; ++c) g.pin[c] = column_payload(pd.pay[c], nullptr, 0, g.pin[c].width);
-    const RunArgs ra{run_off, run_cnt, (uint32_t)n_tiles, 1u << pbits};
+    const RunArgs ra{run_off, run_cnt, (uint32_t)n_tiles, 1u << pbits, 1u};  // group: set by probe_runs
     probe_runs(t, pd.keys, ra, g, s, tile_ctr);
     SJ_CUDA_TRY(cudaGetLastError());
     return SJ_OK;
